@@ -1,0 +1,169 @@
+/*
+ * periodicflow_b200.h -- C ABI of the B200 backend of periodicflow's
+ * right-hand-side and time-stepping path.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, int status codes
+ * (PF_OK == 0).  Complex arrays are interleaved (re, im) doubles in the
+ * reference's layout: spectral fields (comp, n0, n1, n2/2+1) in 3D and
+ * (comp, n0, n1/2+1) in 2D; physical fields (comp, n0, n1[, n2]).  A handle
+ * is not thread-safe; all of its work is ordered on one CUDA stream.
+ *
+ * Reference interfaces replaced (paths inside the periodic-flow project):
+ *   Solver.__init__            src/periodicflow/simulation.py:56-114
+ *   SpaceSolver.__init__       src/periodicflow/space_solver.py:107-150
+ *   FourierSpace.__init__      src/periodicflow/basis.py:87-145
+ *   Solver.initialize          src/periodicflow/simulation.py:161-180
+ *   initialize_velocity        src/periodicflow/space_solver.py:180-213
+ *   forward / backward         src/periodicflow/space_solver.py:215-225
+ *   set_linear_operator        src/periodicflow/simulation.py:182-184
+ *   update_linear_operator     src/periodicflow/time_integrator.py:31-33
+ *   set_correlation_function   src/periodicflow/simulation.py:186-187
+ *   random_fields              src/periodicflow/space_solver.py:227-238
+ *   Solver.solve loop body     src/periodicflow/simulation.py:205-217
+ *   compute_rhs                src/periodicflow/space_solver.py:302-310
+ *   TimeIntegrator.stepping    src/periodicflow/time_integrator.py:36-318
+ *   math.cross/curl/apply_linear_operator/leray_projection
+ *                              src/periodicflow/math.py:4-100
+ *   _symmetrize/_noise_divergence
+ *                              src/periodicflow/space_solver.py:15-64
+ */
+#ifndef PERIODICFLOW_B200_H
+#define PERIODICFLOW_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define PF_OK 0
+#define PF_ERR_INVALID 1     /* bad argument (the reference raises ValueError) */
+#define PF_ERR_CUDA 2        /* CUDA runtime error */
+#define PF_ERR_UNSUPPORTED 3 /* valid in the reference, not built here */
+#define PF_ERR_NOMEM 4
+
+/* integrators: registry names of time_integrator.py:36,93,161,213,278 */
+#define PF_EXPLICIT_PC 0
+#define PF_IMPLICIT_PC 1
+#define PF_RK2 2
+#define PF_RK3 3
+#define PF_RK4 4
+
+#define PF_NOISE_THERMAL 0    /* space_solver.py:254-259 */
+#define PF_NOISE_CORRELATED 1 /* space_solver.py:261-265 */
+
+#define PF_NOISE_SRC_PHILOX 1   /* counter-based, Hermitian-symmetric draws */
+#define PF_NOISE_SRC_INJECTED 2 /* caller supplies w1, w2 every step */
+
+#define PF_DEALIAS_TRUNCATE 0 /* '2/3' / 'truncate' (basis.py:135-136) */
+#define PF_DEALIAS_PAD 1      /* '3/2' / 'pad' (basis.py:133-134) */
+
+#define PF_FP32 0
+#define PF_FP64 1
+
+typedef struct pf_config {
+  int dim;                /* 2 or 3 */
+  int n[3];               /* grid points per axis (power of two, 4..1024) */
+  double domain[3][2];    /* (start, end) per axis */
+  int is_nonlinear;       /* simulation.py:61 */
+  int integrator;         /* PF_EXPLICIT_PC .. PF_RK4 */
+  double viscosity;       /* L = -viscosity |k|^2 (space_solver.py:147) */
+  int noise_type;         /* PF_NOISE_THERMAL / PF_NOISE_CORRELATED */
+  double noise_mag;       /* 0 disables the noise term */
+  int dealias;            /* PF_DEALIAS_TRUNCATE */
+  int mask_nyquist;       /* zero Nyquist modes of the nonlinear term */
+  int precision;          /* PF_FP32 / PF_FP64 */
+  double dt;
+  unsigned long long seed;/* Philox key */
+  int noise_source;       /* PF_NOISE_SRC_PHILOX / PF_NOISE_SRC_INJECTED */
+  double forcing_eps;     /* >0: linear band forcing at injection rate eps */
+  double forcing_kf;      /* forced band 0 < |k| <= kf */
+  double cfl;             /* >0: dt = cfl / max(sum_i |u_i| / dx_i) each step */
+  int fused;              /* 1: fused pencil passes where built; 0: per-operator */
+} pf_config;
+
+typedef struct pf_solver pf_solver;
+
+/* Fill cfg with the reference's defaults (simulation.py:56-79; dealias 2/3). */
+int pf_config_default(pf_config* cfg);
+
+/* Create a solver on the current CUDA device; state is zero. */
+int pf_create(const pf_config* cfg, pf_solver** out);
+int pf_destroy(pf_solver* h);
+/* Order the handle's work on this cudaStream_t (NULL = legacy default). */
+int pf_set_stream(pf_solver* h, void* stream);
+/* Message of the last failing call on h (static text when h is NULL). */
+const char* pf_last_error(const pf_solver* h);
+
+/* Extents: spectral modes per component, physical points per component,
+ * noise components (d*d thermal, d correlated). */
+int pf_sizes(const pf_solver* h, long long* nspec, long long* nphys, int* ncomp);
+
+/* State transfer.  `where` = 0: host pointer, 1: device pointer.
+ * Fourier data are complex128 (2 doubles per value), physical data float64. */
+int pf_set_fourier(pf_solver* h, const double* u_hat, int where);
+int pf_get_fourier(pf_solver* h, double* u_hat, int where);
+/* physical -> spectral with the normalised forward transform (V.forward) */
+int pf_set_physical(pf_solver* h, const double* u, int where);
+/* spectral -> physical with the backward transform (V.backward) */
+int pf_get_physical(pf_solver* h, double* u, int where);
+/* initialize(): zero the k = 0 mode (space_solver.py:208-209) */
+int pf_mask_zero_mode(pf_solver* h);
+/* initialize(project=True): Leray projection of the state (simulation.py:170-176) */
+int pf_project(pf_solver* h);
+
+/* L(k) and C(k) as float64 arrays of the scalar spectral shape; NULL restores
+ * the defaults (-viscosity |k|^2 and zero). */
+int pf_set_linear_operator(pf_solver* h, const double* L, int where);
+int pf_set_correlation(pf_solver* h, const double* C, int where);
+
+/* Noise of the next step for PF_NOISE_SRC_INJECTED: w1, w2 as stored by the
+ * reference after random_fields() (normal factor applied), complex128 of shape
+ * (ncomp, spectral). */
+int pf_inject_noise(pf_solver* h, const double* w1, const double* w2, int where);
+
+/* Advance nsteps full time steps (all stages) on the device. */
+int pf_step(pf_solver* h, int nsteps);
+
+/* Time, step counter and current dt (synchronises the stream). */
+int pf_get_time(pf_solver* h, double* t, long long* step, double* dt);
+/* Set time / step counter (restart). */
+int pf_set_time(pf_solver* h, double t, long long step);
+/* Kinetic energy and enstrophy of the current state (FP64 reductions). */
+int pf_energy(pf_solver* h, double* energy, double* enstrophy);
+/* Per-step E, Z recorded by pf_step since the last call (2 doubles per
+ * step, at most max_steps); returns the count in *count. */
+int pf_history(pf_solver* h, double* out, int max_steps, int* count);
+/* Record E, Z of every step inside pf_step (0/1). */
+int pf_record_history(pf_solver* h, int enable);
+/* Shell spectrum E(k), nbins bins of width 2 pi / L0. */
+int pf_spectrum(pf_solver* h, double* out, int nbins);
+
+/* ---- operators on device arrays (math.py / space_solver.py kernels) ------
+ * Arrays are device pointers of element type double (PF_FP64) or float
+ * (PF_FP32); complex arrays interleaved.  shape = spatial extents of one
+ * component (dim entries).  Semantics are those of the reference functions. */
+int pf_op_cross(int precision, int dim, const long long* shape, void* c, const void* a,
+                const void* b, void* stream);
+int pf_op_curl(int precision, int dim, const long long* shape, void* c, const void* k,
+               const void* a, void* stream);
+int pf_op_apply_linear_operator(int precision, int dim, const long long* shape, void* Lu,
+                                const void* L, const void* u, void* stream);
+int pf_op_leray_projection(int precision, int dim, const long long* shape, void* u,
+                           const void* k, const void* k_over_k2, void* p_hat, void* stream);
+int pf_op_symmetrize(int precision, int dim, const long long* shape, void* w_sym,
+                     const void* w, void* stream);
+int pf_op_noise_divergence(int precision, int dim, const long long* shape, void* noise,
+                           const void* w_sym, const void* k, void* stream);
+/* One stage of an integrator on device arrays (TimeIntegrator.stepping):
+ * unew updated in place; for PF_IMPLICIT_PC the last stage overwrites
+ * rhs_linear with L u0 as the reference does.  L may be NULL for integrators
+ * that do not use it. */
+int pf_op_stepping(int precision, int integrator, int stage, double dt, long long n,
+                   void* unew, const void* u0, const void* rhs_nonlinear, void* rhs_linear,
+                   const void* forcing, const void* noise, const void* L,
+                   long long n_per_comp, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PERIODICFLOW_B200_H */

@@ -1,0 +1,716 @@
+// C-ABI solver: owns the device state of one periodic box and runs the
+// reference's time loop (simulation.py:205-217) on one CUDA stream.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/periodicflow_b200.h"
+#include "pf_fused.h"
+#include "pf_kernels.h"
+
+using namespace pf;
+
+struct pf_solver {
+  pf_config cfg;
+  Geo g;
+  int d = 0, ncomp = 0, prec = 0;
+  size_t rsz = 4;  // sizeof(real)
+  cudaStream_t st = nullptr;
+  void* uhat = nullptr;   // d * nspec complex
+  void* u0 = nullptr;     // d * nspec complex
+  void* nl = nullptr;     // d * nspec complex
+  void* spec_tmp = nullptr;  // 3 * nspec complex
+  void* phys_u = nullptr; // d * nphys real
+  void* phys_w = nullptr; // (3D: 3, 2D: 1) * nphys real
+  void* lop = nullptr;    // nspec real (user L)
+  void* corr = nullptr;   // nspec real (user C)
+  void* winj = nullptr;   // 2 * ncomp * nspec complex
+  double* stage64 = nullptr;  // FP64 staging for transfers
+  size_t stage64_elems = 0;
+  double* dscal = nullptr;
+  unsigned long long* maxbits = nullptr;
+  double* hist_dev = nullptr;  // 2 * kHist doubles
+  int hist_fill = 0;
+  bool record_hist = false;
+  bool noise_ready = false;
+  std::vector<double> hist;
+  long long step = 0;
+  double t = 0.0;
+  FusedPlan* fused = nullptr;
+  std::string err;
+};
+
+static const int kHist = 4096;
+static std::string g_static_err;
+
+static int fail(pf_solver* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  else g_static_err = msg;
+  return code;
+}
+
+#define PF_CUDA(h, call)                                                              \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      return fail(h, PF_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// ---------------------------------------------------------------- conversions
+template <typename R>
+__global__ void k_from64(R* __restrict__ dst, const double* __restrict__ src, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    dst[i] = (R)src[i];
+}
+template <typename R>
+__global__ void k_to64(double* __restrict__ dst, const R* __restrict__ src, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    dst[i] = (double)src[i];
+}
+template <typename R>
+__global__ void k_scale_mask0(cx<R>* u, Geo g, int ncomp) {
+  // zero the k = 0 mode of every component
+  if (blockIdx.x == 0 && threadIdx.x < ncomp) u[threadIdx.x * g.nspec] = czero<cx<R>>();
+}
+template <typename R, int D>
+__global__ void k_project(cx<R>* u, Geo g) {
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < g.nspec;
+       m += (long long)gridDim.x * blockDim.x) {
+    const ModeIdx ix = mode_index(g, m);
+    const KInt<D> ki = kint_of<D>(g, ix);
+    R k[D];
+    double k2 = 0.0;
+    for (int a = 0; a < D; ++a) {
+      const double ka = g.kscale[a] * ki.k[a];
+      k[a] = (R)ka;
+      k2 += ka * ka;
+    }
+    cx<R> v[D];
+    for (int a = 0; a < D; ++a) v[a] = u[a * g.nspec + m];
+    leray<R, D>(v, k, (R)k2);
+    for (int a = 0; a < D; ++a) u[a * g.nspec + m] = v[a];
+  }
+}
+
+static unsigned blocks_for(long long n) {
+  long long b = (n + 255) / 256;
+  if (b > 148 * 16) b = 148 * 16;
+  if (b < 1) b = 1;
+  return (unsigned)b;
+}
+
+// ------------------------------------------------------------ transforms
+template <typename R>
+static cudaError_t backward_inplace(pf_solver* h, cx<R>* X, R* P, int nc) {
+  const Geo& g = h->g;
+  cudaError_t e;
+  if (g.dim == 3) {
+    const long long plane = (long long)g.s[1] * g.nh;
+    e = fft_strided<R>(X, g.n[0], +1, plane, nc, g.nspec, plane, 1.0, h->st);
+    if (e != cudaSuccess) return e;
+    e = fft_strided<R>(X, g.n[1], +1, g.nh, (long long)nc * g.n[0], plane, g.nh, 1.0, h->st);
+    if (e != cudaSuccess) return e;
+    return fft_c2r_last<R>(X, P, g.n[2], (long long)nc * g.n[0] * g.n[1], g.nh, g.n[2], h->st);
+  }
+  e = fft_strided<R>(X, g.n[0], +1, g.nh, nc, g.nspec, g.nh, 1.0, h->st);
+  if (e != cudaSuccess) return e;
+  return fft_c2r_last<R>(X, P, g.n[1], (long long)nc * g.n[0], g.nh, g.n[1], h->st);
+}
+
+template <typename R>
+static cudaError_t forward_into(pf_solver* h, const R* P, cx<R>* X, int nc) {
+  const Geo& g = h->g;
+  const double scale = 1.0 / (double)g.nphys;
+  cudaError_t e;
+  if (g.dim == 3) {
+    const long long plane = (long long)g.s[1] * g.nh;
+    e = fft_r2c_last<R>(P, X, g.n[2], (long long)nc * g.n[0] * g.n[1], g.n[2], g.nh, scale, h->st);
+    if (e != cudaSuccess) return e;
+    e = fft_strided<R>(X, g.n[1], -1, g.nh, (long long)nc * g.n[0], plane, g.nh, 1.0, h->st);
+    if (e != cudaSuccess) return e;
+    return fft_strided<R>(X, g.n[0], -1, plane, nc, g.nspec, plane, 1.0, h->st);
+  }
+  e = fft_r2c_last<R>(P, X, g.n[1], (long long)nc * g.n[0], g.n[1], g.nh, scale, h->st);
+  if (e != cudaSuccess) return e;
+  return fft_strided<R>(X, g.n[0], -1, g.nh, nc, g.nspec, g.nh, 1.0, h->st);
+}
+
+// nonlinear term u x w (unprojected) of the current state into h->nl
+template <typename R>
+static cudaError_t nonlinear_generic(pf_solver* h, bool want_max) {
+  const Geo& g = h->g;
+  cx<R>* tmp = (cx<R>*)h->spec_tmp;
+  cudaError_t e;
+  const int wc = g.dim == 3 ? 3 : 1;
+  e = launch_curl_masked<R>(tmp, (const cx<R>*)h->uhat, g, h->st);
+  if (e != cudaSuccess) return e;
+  e = backward_inplace<R>(h, tmp, (R*)h->phys_w, wc);
+  if (e != cudaSuccess) return e;
+  e = launch_mask_copy<R>(tmp, (const cx<R>*)h->uhat, g, h->d, h->st);
+  if (e != cudaSuccess) return e;
+  e = backward_inplace<R>(h, tmp, (R*)h->phys_u, h->d);
+  if (e != cudaSuccess) return e;
+  if (want_max) {
+    e = cudaMemsetAsync(h->maxbits, 0, sizeof(unsigned long long), h->st);
+    if (e != cudaSuccess) return e;
+  }
+  e = launch_cross<R>((R*)h->phys_u, (const R*)h->phys_w, g, want_max ? h->maxbits : nullptr,
+                      h->st);
+  if (e != cudaSuccess) return e;
+  return forward_into<R>(h, (const R*)h->phys_u, (cx<R>*)h->nl, h->d);
+}
+
+// ------------------------------------------------------------------ schemes
+static Scheme make_scheme(int integ) {
+  Scheme s;
+  memset(&s, 0, sizeof(s));
+  auto set = [&](int i, double cu0, double cun, double cd, double cL, double cx, double a,
+                 int Lu0, int impl) {
+    s.st[i].cu0 = cu0; s.st[i].cun = cun; s.st[i].cd = cd; s.st[i].cL = cL;
+    s.st[i].cx = cx; s.st[i].a = a; s.st[i].L_on_u0 = Lu0; s.st[i].implicit = impl;
+  };
+  const double rh = std::sqrt(0.5);
+  switch (integ) {
+    case PF_EXPLICIT_PC:  // time_integrator.py:45-56
+      s.nstages = 2;
+      set(0, 1, 0, 0.5, 0.5, rh, 0.0, 0, 0);
+      set(1, 1, 0, 1.0, 1.0, rh, 1.0, 0, 0);
+      break;
+    case PF_IMPLICIT_PC:  // time_integrator.py:102-119
+      s.nstages = 2;
+      set(0, 1, 0, 0.5, 0.0, rh, 0.0, 0, 1);
+      set(1, 1, 0, 1.0, 0.5, rh, 1.0, 1, 1);
+      break;
+    case PF_RK2:  // time_integrator.py:170-180 (noise_factor supplied as zeros)
+      s.nstages = 2;
+      set(0, 0.0, 1.0, 1.0, 1.0, 0, 0.0, 0, 0);
+      set(1, 0.5, 0.5, 0.5, 0.5, 0, 0.0, 0, 0);
+      break;
+    case PF_RK3: {  // time_integrator.py:222-241
+      s.nstages = 3;
+      const double r2 = std::sqrt(2.0), r3 = std::sqrt(3.0);
+      set(0, 0.0, 1.0, 1.0, 1.0, 1.0, (2 * r2 + r3) / 5, 0, 0);
+      set(1, 0.75, 0.25, 0.25, 0.25, 0.25, (-4 * r2 + 3 * r3) / 5, 0, 0);
+      set(2, 1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0, (r2 - 2 * r3) / 10, 0, 0);
+      break;
+    }
+    default:  // PF_RK4, time_integrator.py:287-293
+      s.nstages = 4;
+      set(0, 1, 0, 0.25, 0.25, 0, 0.0, 0, 0);
+      set(1, 1, 0, 1.0 / 3.0, 1.0 / 3.0, 0, 0.0, 0, 0);
+      set(2, 1, 0, 0.5, 0.5, 0, 0.0, 0, 0);
+      set(3, 1, 0, 1.0, 1.0, 0, 0.0, 0, 0);
+      break;
+  }
+  return s;
+}
+
+static double noise_norm(const pf_solver* h) {
+  return 1.0 / std::sqrt((double)h->g.nphys) / std::sqrt(2.0 - 2.0 / h->d);
+}
+
+static int noise_src(const pf_solver* h) {
+  if (h->cfg.noise_mag == 0.0) return kNoiseNone;
+  return h->cfg.noise_source == PF_NOISE_SRC_INJECTED ? kNoiseInjected : kNoisePhilox;
+}
+
+// --------------------------------------------------------------- one step
+template <typename R>
+static int step_generic(pf_solver* h) {
+  const Geo& g = h->g;
+  const Scheme sc = make_scheme(h->cfg.integrator);
+  const bool cfl = h->cfg.cfl > 0.0;
+  const bool forcing = h->cfg.forcing_eps > 0.0;
+  for (int s = 0; s < sc.nstages; ++s) {
+    if (h->cfg.is_nonlinear) {
+      if (h->fused && h->cfg.fused) {
+        PF_CUDA(h, fused_nonlinear(h->fused, h->uhat, h->nl, (s == 0 && cfl) ? h->maxbits : nullptr,
+                                   h->st));
+      } else {
+        PF_CUDA(h, nonlinear_generic<R>(h, s == 0 && cfl));
+      }
+      if (s == 0 && cfl) PF_CUDA(h, launch_set_dt(h->dscal, h->maxbits, h->cfg.cfl, h->st));
+    } else if (s == 0 && cfl) {
+      return fail(h, PF_ERR_UNSUPPORTED, "CFL-adaptive dt needs the nonlinear term");
+    }
+    if (forcing)
+      PF_CUDA(h, launch_band_energy<R>((const cx<R>*)h->uhat, g,
+                                       h->cfg.forcing_kf * h->cfg.forcing_kf, h->dscal, h->st));
+    UpdateArgs<R> A;
+    memset(&A, 0, sizeof(A));
+    A.uhat = (cx<R>*)h->uhat;
+    A.u0 = (cx<R>*)h->u0;
+    A.nl = h->cfg.is_nonlinear ? (const cx<R>*)h->nl : nullptr;
+    A.lop = (const R*)h->lop;
+    A.corr = (const R*)h->corr;
+    A.winj = (const cx<R>*)h->winj;
+    A.dscal = h->dscal;
+    A.diag = (h->record_hist && s == sc.nstages - 1) ? h->hist_dev + 2 * h->hist_fill : nullptr;
+    A.g = g;
+    A.coef = sc.st[s];
+    A.nu = h->cfg.viscosity;
+    A.noise_mag = h->cfg.noise_mag;
+    A.noise_norm = noise_norm(h);
+    A.f_eps = h->cfg.forcing_eps;
+    A.f_kf2 = h->cfg.forcing_kf * h->cfg.forcing_kf;
+    A.seed = h->cfg.seed;
+    A.step = (uint64_t)(h->step + 1);
+    A.noise_src = noise_src(h);
+    A.noise_type = h->cfg.noise_type;
+    A.save_u0 = s == 0;
+    A.nyq_mask = h->cfg.mask_nyquist;
+    A.forcing = forcing;
+    PF_CUDA(h, launch_update<R>(A, h->ncomp, h->st));
+  }
+  if (!cfl) PF_CUDA(h, launch_advance_time(h->dscal, 1, h->st));
+  return PF_OK;
+}
+
+template <typename R>
+static int step_stokes(pf_solver* h, int nsteps) {
+  StokesArgs<R> A;
+  memset(&A, 0, sizeof(A));
+  A.uhat = (cx<R>*)h->uhat;
+  A.lop = (const R*)h->lop;
+  A.corr = (const R*)h->corr;
+  A.winj = (const cx<R>*)h->winj;
+  A.g = h->g;
+  A.scheme = make_scheme(h->cfg.integrator);
+  A.dt = h->cfg.dt;
+  A.nu = h->cfg.viscosity;
+  A.noise_mag = h->cfg.noise_mag;
+  A.noise_norm = noise_norm(h);
+  A.seed = h->cfg.seed;
+  A.step0 = (uint64_t)(h->step + 1);
+  A.nsteps = nsteps;
+  A.noise_src = noise_src(h);
+  A.noise_type = h->cfg.noise_type;
+  PF_CUDA(h, launch_stokes<R>(A, h->ncomp, h->st));
+  PF_CUDA(h, launch_advance_time(h->dscal, nsteps, h->st));
+  return PF_OK;
+}
+
+static int flush_hist(pf_solver* h) {
+  if (h->hist_fill == 0) return PF_OK;
+  std::vector<double> tmp(2 * h->hist_fill);
+  PF_CUDA(h, cudaMemcpyAsync(tmp.data(), h->hist_dev, sizeof(double) * tmp.size(),
+                             cudaMemcpyDeviceToHost, h->st));
+  PF_CUDA(h, cudaStreamSynchronize(h->st));
+  h->hist.insert(h->hist.end(), tmp.begin(), tmp.end());
+  h->hist_fill = 0;
+  PF_CUDA(h, cudaMemsetAsync(h->hist_dev, 0, sizeof(double) * 2 * kHist, h->st));
+  return PF_OK;
+}
+
+template <typename R>
+static int step_impl(pf_solver* h, int nsteps) {
+  const bool stokes_fast = !h->cfg.is_nonlinear && h->cfg.forcing_eps <= 0.0 &&
+                           h->cfg.cfl <= 0.0;
+  const bool injected = noise_src(h) == kNoiseInjected;
+  if (injected && (nsteps > 1 || !h->noise_ready))
+    return fail(h, PF_ERR_INVALID,
+                "injected noise: call pf_inject_noise before every single pf_step(h, 1)");
+  int done = 0;
+  while (done < nsteps) {
+    int chunk = nsteps - done;
+    if (h->record_hist) chunk = 1;
+    if (stokes_fast) {
+      int rc = step_stokes<R>(h, chunk);
+      if (rc) return rc;
+      if (h->record_hist)
+        PF_CUDA(h, launch_energy<R>((const cx<R>*)h->uhat, h->g, h->hist_dev + 2 * h->hist_fill,
+                                    h->st));
+    } else {
+      chunk = 1;
+      int rc = step_generic<R>(h);
+      if (rc) return rc;
+    }
+    h->step += chunk;
+    done += chunk;
+    if (h->record_hist) {
+      h->hist_fill += 1;
+      if (h->hist_fill == kHist) {
+        int rc = flush_hist(h);
+        if (rc) return rc;
+      }
+    }
+  }
+  h->noise_ready = false;
+  return PF_OK;
+}
+
+// ================================================================ C ABI
+extern "C" {
+
+int pf_config_default(pf_config* c) {
+  if (!c) return fail(nullptr, PF_ERR_INVALID, "pf_config_default: null config");
+  memset(c, 0, sizeof(*c));
+  c->dim = 3;
+  c->n[0] = c->n[1] = c->n[2] = 64;
+  for (int i = 0; i < 3; ++i) { c->domain[i][0] = 0.0; c->domain[i][1] = 2.0 * M_PI; }
+  c->is_nonlinear = 1;
+  c->integrator = PF_RK2;
+  c->viscosity = 1e-3;
+  c->noise_type = PF_NOISE_THERMAL;
+  c->noise_mag = 0.0;
+  c->dealias = PF_DEALIAS_TRUNCATE;
+  c->mask_nyquist = 0;
+  c->precision = PF_FP32;
+  c->dt = 1e-3;
+  c->seed = 0;
+  c->noise_source = PF_NOISE_SRC_PHILOX;
+  c->forcing_kf = 2.5;
+  c->fused = 1;
+  return PF_OK;
+}
+
+const char* pf_last_error(const pf_solver* h) {
+  return h ? h->err.c_str() : g_static_err.c_str();
+}
+
+static int validate(const pf_config* c) {
+  if (c->dim != 2 && c->dim != 3)
+    return fail(nullptr, PF_ERR_INVALID, "NS solver only supports 2D and 3D problems.");
+  for (int a = 0; a < c->dim; ++a) {
+    if (!fft_length_supported(c->n[a]))
+      return fail(nullptr, PF_ERR_UNSUPPORTED,
+                  "grid size " + std::to_string(c->n[a]) +
+                      " not built: powers of two from 4 to 1024 are supported");
+    if (!(c->domain[a][1] > c->domain[a][0]))
+      return fail(nullptr, PF_ERR_INVALID, "Invalid domain.");
+  }
+  if (c->integrator < PF_EXPLICIT_PC || c->integrator > PF_RK4)
+    return fail(nullptr, PF_ERR_INVALID, "Time integrator not found.");
+  if (c->noise_type != PF_NOISE_THERMAL && c->noise_type != PF_NOISE_CORRELATED)
+    return fail(nullptr, PF_ERR_INVALID,
+                "Invalid noise type. Options are 'thermal' or 'correlated'.");
+  if (c->dealias != PF_DEALIAS_TRUNCATE)
+    return fail(nullptr, PF_ERR_UNSUPPORTED, "3/2 padding dealiasing is not built");
+  if (c->precision != PF_FP32 && c->precision != PF_FP64)
+    return fail(nullptr, PF_ERR_INVALID, "precision must be PF_FP32 or PF_FP64");
+  if (!(c->dt > 0.0)) return fail(nullptr, PF_ERR_INVALID, "dt must be positive");
+  return PF_OK;
+}
+
+int pf_create(const pf_config* cfg, pf_solver** out) {
+  if (!cfg || !out) return fail(nullptr, PF_ERR_INVALID, "pf_create: null argument");
+  *out = nullptr;
+  int rc = validate(cfg);
+  if (rc) return rc;
+  cudaError_t ce = ensure_tables();
+  if (ce != cudaSuccess)
+    return fail(nullptr, PF_ERR_CUDA, std::string("twiddle tables: ") + cudaGetErrorString(ce));
+  pf_solver* h = new pf_solver();
+  h->cfg = *cfg;
+  h->d = cfg->dim;
+  h->prec = cfg->precision;
+  h->rsz = h->prec == PF_FP64 ? 8 : 4;
+  h->ncomp = cfg->noise_type == PF_NOISE_THERMAL ? h->d * h->d : h->d;
+  Geo& g = h->g;
+  memset(&g, 0, sizeof(g));
+  g.dim = h->d;
+  g.n[2] = 1;
+  for (int a = 0; a < h->d; ++a) {
+    g.n[a] = cfg->n[a];
+    g.kscale[a] = 2.0 * M_PI / (cfg->domain[a][1] - cfg->domain[a][0]);
+    g.kmax[a] = (cfg->n[a] - 1) / 3;
+    g.s[a] = cfg->n[a];
+  }
+  g.nh = cfg->n[h->d - 1] / 2 + 1;
+  g.s[h->d - 1] = g.nh;
+  g.nspec = 1;
+  g.nphys = 1;
+  for (int a = 0; a < h->d; ++a) { g.nspec *= g.s[a]; g.nphys *= g.n[a]; }
+  const size_t cb = 2 * h->rsz;  // complex bytes
+  auto alloc = [&](void** p, size_t bytes) -> bool {
+    if (cudaMalloc(p, bytes) != cudaSuccess) return false;
+    return cudaMemset(*p, 0, bytes) == cudaSuccess;
+  };
+  const int wc = h->d == 3 ? 3 : 1;
+  h->stage64_elems = std::max((size_t)(2 * h->d * g.nspec), (size_t)(h->d * g.nphys));
+  h->stage64_elems = std::max(h->stage64_elems, (size_t)(4 * h->ncomp * g.nspec));
+  bool ok = alloc(&h->uhat, cb * h->d * g.nspec) && alloc(&h->u0, cb * h->d * g.nspec) &&
+            alloc(&h->spec_tmp, cb * 3 * g.nspec) &&
+            alloc((void**)&h->stage64, sizeof(double) * h->stage64_elems) &&
+            alloc((void**)&h->dscal, sizeof(double) * kScalCount) &&
+            alloc((void**)&h->maxbits, sizeof(unsigned long long)) &&
+            alloc((void**)&h->hist_dev, sizeof(double) * 2 * kHist);
+  if (ok && cfg->is_nonlinear) {
+    ok = alloc(&h->nl, cb * h->d * g.nspec) && alloc(&h->phys_u, h->rsz * h->d * g.nphys) &&
+         alloc(&h->phys_w, h->rsz * wc * g.nphys);
+  }
+  if (ok && cfg->noise_mag != 0.0 && cfg->noise_source == PF_NOISE_SRC_INJECTED)
+    ok = alloc(&h->winj, cb * 2 * h->ncomp * g.nspec);
+  if (!ok) {
+    std::string m = std::string("device allocation failed: ") + cudaGetErrorString(cudaGetLastError());
+    pf_destroy(h);
+    return fail(nullptr, PF_ERR_NOMEM, m);
+  }
+  double dt0 = cfg->dt;
+  cudaMemcpy(h->dscal + kScalDt, &dt0, sizeof(double), cudaMemcpyHostToDevice);
+  if (cfg->is_nonlinear && cfg->fused) {
+    h->fused = fused_create(g, h->prec, cfg->dealias);  // nullptr when no fused path fits
+  }
+  *out = h;
+  return PF_OK;
+}
+
+int pf_destroy(pf_solver* h) {
+  if (!h) return PF_OK;
+  void* ptrs[] = {h->uhat, h->u0, h->nl, h->spec_tmp, h->phys_u, h->phys_w, h->lop,
+                  h->corr, h->winj, h->stage64, h->dscal, h->maxbits, h->hist_dev};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (h->fused) fused_destroy(h->fused);
+  delete h;
+  return PF_OK;
+}
+
+int pf_set_stream(pf_solver* h, void* stream) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  h->st = (cudaStream_t)stream;
+  return PF_OK;
+}
+
+int pf_sizes(const pf_solver* h, long long* nspec, long long* nphys, int* ncomp) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  if (nspec) *nspec = h->g.nspec;
+  if (nphys) *nphys = h->g.nphys;
+  if (ncomp) *ncomp = h->ncomp;
+  return PF_OK;
+}
+
+// copy n doubles from (host|device) src into the FP64 staging buffer
+static int stage_in(pf_solver* h, const double* src, size_t n, int where) {
+  PF_CUDA(h, cudaMemcpyAsync(h->stage64, src, sizeof(double) * n,
+                             where ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->st));
+  return PF_OK;
+}
+static int stage_out(pf_solver* h, double* dst, size_t n, int where) {
+  PF_CUDA(h, cudaMemcpyAsync(dst, h->stage64, sizeof(double) * n,
+                             where ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->st));
+  PF_CUDA(h, cudaStreamSynchronize(h->st));
+  return PF_OK;
+}
+static cudaError_t convert_in(pf_solver* h, void* dst, size_t n) {
+  if (h->prec == PF_FP64)
+    return cudaMemcpyAsync(dst, h->stage64, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->st);
+  k_from64<float><<<blocks_for(n), 256, 0, h->st>>>((float*)dst, h->stage64, (long long)n);
+  return cudaGetLastError();
+}
+static cudaError_t convert_out(pf_solver* h, const void* src, size_t n) {
+  if (h->prec == PF_FP64)
+    return cudaMemcpyAsync(h->stage64, src, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->st);
+  k_to64<float><<<blocks_for(n), 256, 0, h->st>>>(h->stage64, (const float*)src, (long long)n);
+  return cudaGetLastError();
+}
+
+int pf_set_fourier(pf_solver* h, const double* u_hat, int where) {
+  if (!h || !u_hat) return fail(h, PF_ERR_INVALID, "pf_set_fourier: null argument");
+  const size_t n = 2 * (size_t)h->d * h->g.nspec;
+  int rc = stage_in(h, u_hat, n, where);
+  if (rc) return rc;
+  PF_CUDA(h, convert_in(h, h->uhat, n));
+  PF_CUDA(h, cudaStreamSynchronize(h->st));
+  return PF_OK;
+}
+
+int pf_get_fourier(pf_solver* h, double* u_hat, int where) {
+  if (!h || !u_hat) return fail(h, PF_ERR_INVALID, "pf_get_fourier: null argument");
+  const size_t n = 2 * (size_t)h->d * h->g.nspec;
+  PF_CUDA(h, convert_out(h, h->uhat, n));
+  return stage_out(h, u_hat, n, where);
+}
+
+int pf_set_physical(pf_solver* h, const double* u, int where) {
+  if (!h || !u) return fail(h, PF_ERR_INVALID, "pf_set_physical: null argument");
+  const size_t n = (size_t)h->d * h->g.nphys;
+  void* phys = h->phys_u;
+  void* own = nullptr;
+  if (!phys) {
+    PF_CUDA(h, cudaMalloc(&own, h->rsz * n));
+    phys = own;
+  }
+  int rc = stage_in(h, u, n, where);
+  if (!rc) {
+    cudaError_t e = convert_in(h, phys, n);
+    if (e == cudaSuccess)
+      e = h->prec == PF_FP64 ? forward_into<double>(h, (const double*)phys, (double2*)h->uhat, h->d)
+                             : forward_into<float>(h, (const float*)phys, (float2*)h->uhat, h->d);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+    if (e != cudaSuccess) rc = fail(h, PF_ERR_CUDA, std::string("pf_set_physical: ") + cudaGetErrorString(e));
+  }
+  if (own) cudaFree(own);
+  return rc;
+}
+
+int pf_get_physical(pf_solver* h, double* u, int where) {
+  if (!h || !u) return fail(h, PF_ERR_INVALID, "pf_get_physical: null argument");
+  const size_t n = (size_t)h->d * h->g.nphys;
+  void* phys = h->phys_u;
+  void* own = nullptr;
+  if (!phys) {
+    PF_CUDA(h, cudaMalloc(&own, h->rsz * n));
+    phys = own;
+  }
+  const size_t cb = 2 * h->rsz;
+  cudaError_t e = cudaMemcpyAsync(h->spec_tmp, h->uhat, cb * h->d * h->g.nspec,
+                                  cudaMemcpyDeviceToDevice, h->st);
+  if (e == cudaSuccess)
+    e = h->prec == PF_FP64
+            ? backward_inplace<double>(h, (double2*)h->spec_tmp, (double*)phys, h->d)
+            : backward_inplace<float>(h, (float2*)h->spec_tmp, (float*)phys, h->d);
+  if (e == cudaSuccess) e = convert_out(h, phys, n);
+  int rc = PF_OK;
+  if (e != cudaSuccess) rc = fail(h, PF_ERR_CUDA, std::string("pf_get_physical: ") + cudaGetErrorString(e));
+  if (!rc) rc = stage_out(h, u, n, where);
+  if (own) cudaFree(own);
+  return rc;
+}
+
+int pf_mask_zero_mode(pf_solver* h) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  if (h->prec == PF_FP64) k_scale_mask0<double><<<1, 32, 0, h->st>>>((double2*)h->uhat, h->g, h->d);
+  else k_scale_mask0<float><<<1, 32, 0, h->st>>>((float2*)h->uhat, h->g, h->d);
+  PF_CUDA(h, cudaGetLastError());
+  return PF_OK;
+}
+
+int pf_project(pf_solver* h) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  const unsigned b = blocks_for(h->g.nspec);
+  if (h->prec == PF_FP64) {
+    if (h->d == 3) k_project<double, 3><<<b, 256, 0, h->st>>>((double2*)h->uhat, h->g);
+    else k_project<double, 2><<<b, 256, 0, h->st>>>((double2*)h->uhat, h->g);
+  } else {
+    if (h->d == 3) k_project<float, 3><<<b, 256, 0, h->st>>>((float2*)h->uhat, h->g);
+    else k_project<float, 2><<<b, 256, 0, h->st>>>((float2*)h->uhat, h->g);
+  }
+  PF_CUDA(h, cudaGetLastError());
+  return PF_OK;
+}
+
+static int set_scalar_field(pf_solver* h, void** slot, const double* src, int where) {
+  const size_t n = (size_t)h->g.nspec;
+  if (!src) {
+    if (*slot) cudaFree(*slot);
+    *slot = nullptr;
+    return PF_OK;
+  }
+  if (!*slot) PF_CUDA(h, cudaMalloc(slot, h->rsz * n));
+  int rc = stage_in(h, src, n, where);
+  if (rc) return rc;
+  PF_CUDA(h, convert_in(h, *slot, n));
+  PF_CUDA(h, cudaStreamSynchronize(h->st));
+  return PF_OK;
+}
+
+int pf_set_linear_operator(pf_solver* h, const double* L, int where) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  return set_scalar_field(h, &h->lop, L, where);
+}
+
+int pf_set_correlation(pf_solver* h, const double* C, int where) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  return set_scalar_field(h, &h->corr, C, where);
+}
+
+int pf_inject_noise(pf_solver* h, const double* w1, const double* w2, int where) {
+  if (!h || !w1 || !w2) return fail(h, PF_ERR_INVALID, "pf_inject_noise: null argument");
+  if (!h->winj)
+    return fail(h, PF_ERR_INVALID,
+                "pf_inject_noise: solver was not created with PF_NOISE_SRC_INJECTED and noise_mag != 0");
+  const size_t n = 2 * (size_t)h->ncomp * h->g.nspec;  // doubles per field
+  int rc = stage_in(h, w1, n, where);
+  if (rc) return rc;
+  PF_CUDA(h, convert_in(h, h->winj, n));
+  rc = stage_in(h, w2, n, where);
+  if (rc) return rc;
+  PF_CUDA(h, convert_in(h, (char*)h->winj + h->rsz * n, n));
+  PF_CUDA(h, cudaStreamSynchronize(h->st));
+  h->noise_ready = true;
+  return PF_OK;
+}
+
+int pf_step(pf_solver* h, int nsteps) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  if (nsteps < 0) return fail(h, PF_ERR_INVALID, "nsteps must be >= 0");
+  if (nsteps == 0) return PF_OK;
+  return h->prec == PF_FP64 ? step_impl<double>(h, nsteps) : step_impl<float>(h, nsteps);
+}
+
+int pf_get_time(pf_solver* h, double* t, long long* step, double* dt) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  double sc[kScalCount];
+  PF_CUDA(h, cudaMemcpyAsync(sc, h->dscal, sizeof(sc), cudaMemcpyDeviceToHost, h->st));
+  PF_CUDA(h, cudaStreamSynchronize(h->st));
+  if (t) *t = sc[kScalTime];
+  if (step) *step = h->step;
+  if (dt) *dt = sc[kScalDt];
+  return PF_OK;
+}
+
+int pf_set_time(pf_solver* h, double t, long long step) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  PF_CUDA(h, cudaMemcpyAsync(h->dscal + kScalTime, &t, sizeof(double), cudaMemcpyHostToDevice, h->st));
+  PF_CUDA(h, cudaStreamSynchronize(h->st));
+  h->step = step;
+  return PF_OK;
+}
+
+int pf_energy(pf_solver* h, double* energy, double* enstrophy) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  double* tmp = h->dscal + 4;  // slots 4, 5
+  PF_CUDA(h, cudaMemsetAsync(tmp, 0, 2 * sizeof(double), h->st));
+  cudaError_t e = h->prec == PF_FP64
+                      ? launch_energy<double>((const double2*)h->uhat, h->g, tmp, h->st)
+                      : launch_energy<float>((const float2*)h->uhat, h->g, tmp, h->st);
+  PF_CUDA(h, e);
+  double r[2];
+  PF_CUDA(h, cudaMemcpyAsync(r, tmp, sizeof(r), cudaMemcpyDeviceToHost, h->st));
+  PF_CUDA(h, cudaStreamSynchronize(h->st));
+  if (energy) *energy = r[0];
+  if (enstrophy) *enstrophy = r[1];
+  return PF_OK;
+}
+
+int pf_record_history(pf_solver* h, int enable) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  h->record_hist = enable != 0;
+  return PF_OK;
+}
+
+int pf_history(pf_solver* h, double* out, int max_steps, int* count) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  int rc = flush_hist(h);
+  if (rc) return rc;
+  const int n = (int)(h->hist.size() / 2);
+  const int m = n < max_steps ? n : max_steps;
+  if (out && m > 0) memcpy(out, h->hist.data(), sizeof(double) * 2 * m);
+  if (count) *count = m;
+  h->hist.erase(h->hist.begin(), h->hist.begin() + 2 * m);
+  return PF_OK;
+}
+
+int pf_spectrum(pf_solver* h, double* out, int nbins) {
+  if (!h || !out || nbins <= 0) return fail(h, PF_ERR_INVALID, "pf_spectrum: bad argument");
+  double* tmp = nullptr;
+  PF_CUDA(h, cudaMalloc(&tmp, sizeof(double) * nbins));
+  cudaError_t e = cudaMemsetAsync(tmp, 0, sizeof(double) * nbins, h->st);
+  if (e == cudaSuccess)
+    e = h->prec == PF_FP64
+            ? launch_spectrum<double>((const double2*)h->uhat, h->g, tmp, nbins, h->g.kscale[0], h->st)
+            : launch_spectrum<float>((const float2*)h->uhat, h->g, tmp, nbins, h->g.kscale[0], h->st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, tmp, sizeof(double) * nbins, cudaMemcpyDeviceToHost, h->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return fail(h, PF_ERR_CUDA, std::string("pf_spectrum: ") + cudaGetErrorString(e));
+  return PF_OK;
+}
+
+}  // extern "C"

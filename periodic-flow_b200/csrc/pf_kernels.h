@@ -1,0 +1,63 @@
+// Argument blocks and launchers of the pointwise kernels.
+#pragma once
+#include "pf_internal.h"
+#include "pf_mode.cuh"
+
+namespace pf {
+
+// device scalar slots of a solver
+enum ScalarSlot {
+  kScalDt = 0,      // current dt
+  kScalBandE = 1,   // forcing band energy (2 slots: reduction writes [1], [2])
+  kScalTime = 3,    // simulation time accumulated on the device
+  kScalCount = 8
+};
+
+template <typename R> struct UpdateArgs {
+  cx<R>* uhat;
+  cx<R>* u0;
+  const cx<R>* nl;     // unprojected nonlinear term or nullptr
+  const R* lop;        // user L(k) or nullptr (-nu k^2)
+  const R* corr;       // correlation function C(k) or nullptr (zero)
+  const cx<R>* winj;   // injected w1, w2: (2 * ncomp, nspec) or nullptr
+  const double* dscal; // device scalars
+  double* diag;        // E, Z accumulators or nullptr
+  Geo g;
+  StageCoef coef;
+  double nu, noise_mag, noise_norm, f_eps, f_kf2;
+  uint64_t seed, step;
+  int noise_src, noise_type, save_u0, nyq_mask, forcing;
+};
+
+template <typename R> struct StokesArgs {
+  cx<R>* uhat;
+  const R* lop;
+  const R* corr;
+  const cx<R>* winj;
+  Geo g;
+  Scheme scheme;
+  double dt, nu, noise_mag, noise_norm;
+  uint64_t seed, step0;
+  int nsteps, noise_src, noise_type;
+};
+
+template <typename R> cudaError_t launch_update(const UpdateArgs<R>& A, int ncomp, cudaStream_t st);
+template <typename R> cudaError_t launch_stokes(const StokesArgs<R>& A, int ncomp, cudaStream_t st);
+template <typename R>
+cudaError_t launch_mask_copy(cx<R>* dst, const cx<R>* src, const Geo& g, int ncomp, cudaStream_t st);
+template <typename R>
+cudaError_t launch_curl_masked(cx<R>* dst, const cx<R>* u, const Geo& g, cudaStream_t st);
+template <typename R>
+cudaError_t launch_cross(R* u, const R* w, const Geo& g, unsigned long long* maxbits, cudaStream_t st);
+cudaError_t launch_set_dt(double* dscal, const unsigned long long* maxbits, double cfl, cudaStream_t st);
+cudaError_t launch_advance_time(double* dscal, int n, cudaStream_t st);
+template <typename R>
+cudaError_t launch_band_energy(const cx<R>* u, const Geo& g, double kf2, double* dscal,
+                               cudaStream_t st);
+template <typename R>
+cudaError_t launch_energy(const cx<R>* u, const Geo& g, double* out2, cudaStream_t st);
+template <typename R>
+cudaError_t launch_spectrum(const cx<R>* u, const Geo& g, double* out, int nbins, double kunit,
+                            cudaStream_t st);
+
+}  // namespace pf

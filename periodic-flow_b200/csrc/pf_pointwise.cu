@@ -1,0 +1,475 @@
+// Pointwise kernels of the solver:
+//   * k_update      : one fused stage of any integrator for every mode
+//                     (Leray projection and Nyquist mask of N, linear term,
+//                     noise assembly, forcing, update rule, optional E/Z sums);
+//   * k_stokes      : whole steps of the linear (Stokes) problem with the
+//                     state in registers and in-register Philox noise;
+//   * k_mask_copy / k_curl_masked / k_cross : pieces of the per-operator
+//                     nonlinear term;
+//   * reductions    : forcing-band energy, max |u|/dx for CFL, E and Z,
+//                     shell spectrum.
+#include <cstdio>
+
+#include "pf_kernels.h"
+#include "pf_mode.cuh"
+
+namespace pf {
+
+constexpr int kBlock = 256;
+
+static unsigned grid_for(long long n, int per_block = kBlock, long long cap = 148LL * 16) {
+  long long b = (n + per_block - 1) / per_block;
+  if (b < 1) b = 1;
+  if (b > cap) b = cap;
+  return (unsigned)b;
+}
+
+// FP64 block reduction of two partial sums into gl[0], gl[1].
+PF_D void block_add2(double a, double b, double* gl) {
+  __shared__ double sa[32], sb[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { sa[w] = a; sb[w] = b; }
+  __syncthreads();
+  if (w == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    a = l < nw ? sa[l] : 0.0;
+    b = l < nw ? sb[l] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if (l == 0) { atomicAdd(gl, a); atomicAdd(gl + 1, b); }
+  }
+}
+
+template <typename R, int D> struct ModeK {
+  R k[D];
+  R k2;
+  KInt<D> ki;
+  ModeIdx ix;
+};
+
+template <typename R, int D> PF_D ModeK<R, D> mode_k(const Geo& g, long long m) {
+  ModeK<R, D> r;
+  r.ix = mode_index(g, m);
+  r.ki = kint_of<D>(g, r.ix);
+  double k2 = 0.0;
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    const double ka = g.kscale[a] * (double)r.ki.k[a];
+    r.k[a] = (R)ka;
+    k2 += ka * ka;
+  }
+  r.k2 = (R)k2;
+  return r;
+}
+
+PF_D double half_weight(const Geo& g, const ModeIdx& ix) {
+  const int il = g.dim == 3 ? ix.i2 : ix.i1;
+  const int nl = g.n[g.dim - 1];
+  return (il == 0 || ((nl % 2 == 0) && il == nl / 2)) ? 1.0 : 2.0;
+}
+
+// Normal factor of the noise draws: mask(k != 0) / sqrt(prod N) / sqrt(2 - 2/d)
+// (space_solver.py:143-145), passed in as nf.
+template <typename R, int D, int NC>
+PF_D void load_noise(const UpdateArgs<R>& A, long long m, const ModeK<R, D>& mk_,
+                     cx<R> (&w1)[NC], cx<R> (&w2)[NC]) {
+  if (A.noise_src == kNoiseInjected) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      w1[c] = A.winj[(long long)c * A.g.nspec + m];
+      w2[c] = A.winj[(long long)(NC + c) * A.g.nspec + m];
+    }
+  } else {
+    const DrawSite s = draw_site(A.g, mk_.ix.i0, mk_.ix.i1, mk_.ix.i2);
+    const R nf = mk_.k2 == R(0) ? R(0) : (R)A.noise_norm;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      w1[c] = cscale(draw_value<R>(s, c, A.seed, A.step), nf);
+      w2[c] = cscale(draw_value<R>(s, NC + c, A.seed, A.step), nf);
+    }
+  }
+}
+
+template <typename R, int D, int NC>
+__global__ void __launch_bounds__(kBlock) k_update(UpdateArgs<R> A) {
+  using C = cx<R>;
+  const Geo& g = A.g;
+  const R dt = (R)A.dscal[kScalDt];
+  const R sqdt = (R)sqrt(A.dscal[kScalDt]);
+  R fcoef = R(0);
+  if (A.forcing) {
+    const double ef = A.dscal[kScalBandE];
+    fcoef = ef > 0.0 ? (R)(A.f_eps / (2.0 * ef)) : R(0);
+  }
+  double accE = 0.0, accZ = 0.0;
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < g.nspec;
+       m += (long long)gridDim.x * blockDim.x) {
+    const ModeK<R, D> mk_ = mode_k<R, D>(g, m);
+    C un[D], u0v[D], nv[D], xi[D];
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      un[a] = A.uhat[a * g.nspec + m];
+      u0v[a] = A.save_u0 ? un[a] : A.u0[a * g.nspec + m];
+    }
+    if (A.save_u0) {
+#pragma unroll
+      for (int a = 0; a < D; ++a) A.u0[a * g.nspec + m] = un[a];
+    }
+    // nonlinear term: Leray projection and optional Nyquist mask
+    // (space_solver.py:297-300)
+    if (A.nl) {
+#pragma unroll
+      for (int a = 0; a < D; ++a) nv[a] = A.nl[a * g.nspec + m];
+      leray<R, D>(nv, mk_.k, mk_.k2);
+      if (A.nyq_mask && is_nyquist<D>(g, mk_.ix)) {
+#pragma unroll
+        for (int a = 0; a < D; ++a) nv[a] = czero<C>();
+      }
+    } else {
+#pragma unroll
+      for (int a = 0; a < D; ++a) nv[a] = czero<C>();
+    }
+    // forcing: eps / (2 E_band) u on 0 < |k|^2 <= kf^2
+    if (A.forcing && mk_.k2 > R(0) && (double)mk_.k2 <= A.f_kf2) {
+#pragma unroll
+      for (int a = 0; a < D; ++a) nv[a] = cadd(nv[a], cscale(un[a], fcoef));
+    }
+    // noise
+    if (A.noise_src != kNoiseNone) {
+      C w1[NC], w2[NC];
+      load_noise<R, D, NC>(A, m, mk_, w1, w2);
+      const R corr = A.corr ? A.corr[m] : R(0);
+      noise_term<R, D, NC>(xi, w1, w2, (R)A.coef.a, A.noise_type, mk_.k, mk_.k2, corr, (R)A.noise_mag);
+    } else {
+#pragma unroll
+      for (int a = 0; a < D; ++a) xi[a] = czero<C>();
+    }
+    const R L = A.lop ? A.lop[m] : (R)(-A.nu) * mk_.k2;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      const C r = stage_update<R>(A.coef, dt, sqdt, L, u0v[a], un[a], nv[a], xi[a]);
+      A.uhat[a * g.nspec + m] = r;
+      un[a] = r;
+    }
+    if (A.diag) {
+      double e = 0.0;
+#pragma unroll
+      for (int a = 0; a < D; ++a) e += (double)un[a].x * un[a].x + (double)un[a].y * un[a].y;
+      const double w = half_weight(g, mk_.ix);
+      accE += 0.5 * w * e;
+      accZ += 0.5 * w * e * (double)mk_.k2;
+    }
+  }
+  if (A.diag) block_add2(accE, accZ, A.diag);
+}
+
+// Whole steps of the Stokes problem (no nonlinear term, no forcing): the
+// state of a mode stays in registers across stages and steps.
+template <typename R, int D, int NC>
+__global__ void __launch_bounds__(kBlock) k_stokes(StokesArgs<R> A) {
+  using C = cx<R>;
+  const Geo& g = A.g;
+  const R dt = (R)A.dt;
+  const R sqdt = (R)sqrt(A.dt);
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < g.nspec;
+       m += (long long)gridDim.x * blockDim.x) {
+    const ModeK<R, D> mk_ = mode_k<R, D>(g, m);
+    C u[D];
+#pragma unroll
+    for (int a = 0; a < D; ++a) u[a] = A.uhat[a * g.nspec + m];
+    const R L = A.lop ? A.lop[m] : (R)(-A.nu) * mk_.k2;
+    const R corr = A.corr ? A.corr[m] : R(0);
+    const DrawSite site = draw_site(g, mk_.ix.i0, mk_.ix.i1, mk_.ix.i2);
+    const R nf = mk_.k2 == R(0) ? R(0) : (R)A.noise_norm;
+    for (int s = 0; s < A.nsteps; ++s) {
+      const uint64_t step = A.step0 + (uint64_t)s;
+      C w1[NC], w2[NC];
+      if (A.noise_src == kNoisePhilox) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          w1[c] = cscale(draw_value<R>(site, c, A.seed, step), nf);
+          w2[c] = cscale(draw_value<R>(site, NC + c, A.seed, step), nf);
+        }
+      } else if (A.noise_src == kNoiseInjected) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          w1[c] = A.winj[(long long)c * g.nspec + m];
+          w2[c] = A.winj[(long long)(NC + c) * g.nspec + m];
+        }
+      }
+      C u0[D];
+#pragma unroll
+      for (int a = 0; a < D; ++a) u0[a] = u[a];
+      for (int st = 0; st < A.scheme.nstages; ++st) {
+        const StageCoef& cf = A.scheme.st[st];
+        C xi[D];
+        if (A.noise_src != kNoiseNone) {
+          noise_term<R, D, NC>(xi, w1, w2, (R)cf.a, A.noise_type, mk_.k, mk_.k2, corr,
+                               (R)A.noise_mag);
+        } else {
+#pragma unroll
+          for (int a = 0; a < D; ++a) xi[a] = czero<C>();
+        }
+#pragma unroll
+        for (int a = 0; a < D; ++a)
+          u[a] = stage_update<R>(cf, dt, sqdt, L, u0[a], u[a], czero<C>(), xi[a]);
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < D; ++a) A.uhat[a * g.nspec + m] = u[a];
+  }
+}
+
+// dst = mask_2/3(src), ncomp fields
+template <typename R, int D>
+__global__ void k_mask_copy(cx<R>* __restrict__ dst, const cx<R>* __restrict__ src, Geo g,
+                            int ncomp) {
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < g.nspec;
+       m += (long long)gridDim.x * blockDim.x) {
+    const ModeIdx ix = mode_index(g, m);
+    const bool keep = keep_dealias<D>(g, kint_of<D>(g, ix));
+    for (int c = 0; c < ncomp; ++c)
+      dst[c * g.nspec + m] = keep ? src[c * g.nspec + m] : czero<cx<R>>();
+  }
+}
+
+// dst = mask_2/3(i k x u)  (math.py:31-49)
+template <typename R, int D>
+__global__ void k_curl_masked(cx<R>* __restrict__ dst, const cx<R>* __restrict__ u, Geo g) {
+  using C = cx<R>;
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < g.nspec;
+       m += (long long)gridDim.x * blockDim.x) {
+    const ModeK<R, D> q = mode_k<R, D>(g, m);
+    const bool keep = keep_dealias<D>(g, q.ki);
+    if constexpr (D == 2) {
+      const C a0 = u[m], a1 = u[g.nspec + m];
+      C w = cmuli(csub(cscale(a1, q.k[0]), cscale(a0, q.k[1])));
+      dst[m] = keep ? w : czero<C>();
+    } else {
+      const C a0 = u[m], a1 = u[g.nspec + m], a2 = u[2 * g.nspec + m];
+      C w0 = cmuli(csub(cscale(a2, q.k[1]), cscale(a1, q.k[2])));
+      C w1 = cmuli(csub(cscale(a0, q.k[2]), cscale(a2, q.k[0])));
+      C w2 = cmuli(csub(cscale(a1, q.k[0]), cscale(a0, q.k[1])));
+      dst[m] = keep ? w0 : czero<C>();
+      dst[g.nspec + m] = keep ? w1 : czero<C>();
+      dst[2 * g.nspec + m] = keep ? w2 : czero<C>();
+    }
+  }
+}
+
+// u <- u x w in place (math.py:4-28); optional max of sum |u_i| / dx_i
+template <typename R, int D>
+__global__ void k_cross(R* __restrict__ u, const R* __restrict__ w, Geo g,
+                        unsigned long long* __restrict__ maxbits) {
+  double mx = 0.0;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < g.nphys;
+       p += (long long)gridDim.x * blockDim.x) {
+    if constexpr (D == 2) {
+      const R a0 = u[p], a1 = u[g.nphys + p], b = w[p];
+      if (maxbits) {
+        const double s = fabs((double)a0) * g.n[0] / (2.0 * M_PI / g.kscale[0]) +
+                         fabs((double)a1) * g.n[1] / (2.0 * M_PI / g.kscale[1]);
+        mx = fmax(mx, s);
+      }
+      u[p] = a1 * b;
+      u[g.nphys + p] = -a0 * b;
+    } else {
+      const R a0 = u[p], a1 = u[g.nphys + p], a2 = u[2 * g.nphys + p];
+      const R b0 = w[p], b1 = w[g.nphys + p], b2 = w[2 * g.nphys + p];
+      if (maxbits) {
+        const double s = fabs((double)a0) * g.n[0] * g.kscale[0] / (2.0 * M_PI) +
+                         fabs((double)a1) * g.n[1] * g.kscale[1] / (2.0 * M_PI) +
+                         fabs((double)a2) * g.n[2] * g.kscale[2] / (2.0 * M_PI);
+        mx = fmax(mx, s);
+      }
+      u[p] = a1 * b2 - a2 * b1;
+      u[g.nphys + p] = a2 * b0 - a0 * b2;
+      u[2 * g.nphys + p] = a0 * b1 - a1 * b0;
+    }
+  }
+  if (maxbits) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    // non-negative doubles order like their bit patterns
+    if ((threadIdx.x & 31) == 0) atomicMax(maxbits, (unsigned long long)__double_as_longlong(mx));
+  }
+}
+
+// dscal[dt] = cfl / max, from the double bits written by k_cross
+__global__ void k_set_dt(double* dscal, const unsigned long long* maxbits, double cfl) {
+  const double mx = __longlong_as_double((long long)*maxbits);
+  if (mx > 0.0) dscal[kScalDt] = cfl / mx;
+  dscal[kScalTime] += dscal[kScalDt];
+}
+
+// t += dt, n times (the reference accumulates t step by step, simulation.py:206)
+__global__ void k_advance_time(double* dscal, int n) {
+  for (int i = 0; i < n; ++i) dscal[kScalTime] += dscal[kScalDt];
+}
+
+// E_band = 1/2 sum_{0<|k|^2<=kf^2} w |u|^2  -> dscal[kScalBandE]
+template <typename R, int D>
+__global__ void k_band_energy(const cx<R>* __restrict__ u, Geo g, double kf2, double* dscal) {
+  double acc = 0.0;
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < g.nspec;
+       m += (long long)gridDim.x * blockDim.x) {
+    const ModeK<double, D> q = mode_k<double, D>(g, m);
+    if (q.k2 > 0.0 && q.k2 <= kf2) {
+      double e = 0.0;
+      for (int a = 0; a < D; ++a) {
+        const cx<R> z = u[a * g.nspec + m];
+        e += (double)z.x * z.x + (double)z.y * z.y;
+      }
+      acc += 0.5 * half_weight(g, q.ix) * e;
+    }
+  }
+  block_add2(acc, 0.0, dscal + kScalBandE);
+}
+
+template <typename R, int D>
+__global__ void k_energy(const cx<R>* __restrict__ u, Geo g, double* out2) {
+  double accE = 0.0, accZ = 0.0;
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < g.nspec;
+       m += (long long)gridDim.x * blockDim.x) {
+    const ModeK<double, D> q = mode_k<double, D>(g, m);
+    double e = 0.0;
+    for (int a = 0; a < D; ++a) {
+      const cx<R> z = u[a * g.nspec + m];
+      e += (double)z.x * z.x + (double)z.y * z.y;
+    }
+    const double w = half_weight(g, q.ix);
+    accE += 0.5 * w * e;
+    accZ += 0.5 * w * e * q.k2;
+  }
+  block_add2(accE, accZ, out2);
+}
+
+template <typename R, int D>
+__global__ void k_spectrum(const cx<R>* __restrict__ u, Geo g, double* out, int nbins,
+                           double kunit) {
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < g.nspec;
+       m += (long long)gridDim.x * blockDim.x) {
+    const ModeK<double, D> q = mode_k<double, D>(g, m);
+    double e = 0.0;
+    for (int a = 0; a < D; ++a) {
+      const cx<R> z = u[a * g.nspec + m];
+      e += (double)z.x * z.x + (double)z.y * z.y;
+    }
+    const int b = (int)floor(sqrt(q.k2) / kunit + 0.5);
+    if (b < nbins) atomicAdd(out + b, 0.5 * half_weight(g, q.ix) * e);
+  }
+}
+
+// -------------------------------------------------------------- launchers
+template <typename R>
+cudaError_t launch_update(const UpdateArgs<R>& A, int ncomp, cudaStream_t st) {
+  const unsigned grid = grid_for(A.g.nspec);
+  if (A.g.dim == 3) {
+    if (ncomp == 9) k_update<R, 3, 9><<<grid, kBlock, 0, st>>>(A);
+    else k_update<R, 3, 3><<<grid, kBlock, 0, st>>>(A);
+  } else {
+    if (ncomp == 4) k_update<R, 2, 4><<<grid, kBlock, 0, st>>>(A);
+    else k_update<R, 2, 2><<<grid, kBlock, 0, st>>>(A);
+  }
+  return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_stokes(const StokesArgs<R>& A, int ncomp, cudaStream_t st) {
+  const unsigned grid = grid_for(A.g.nspec, kBlock, 148LL * 64);
+  if (A.g.dim == 3) {
+    if (ncomp == 9) k_stokes<R, 3, 9><<<grid, kBlock, 0, st>>>(A);
+    else k_stokes<R, 3, 3><<<grid, kBlock, 0, st>>>(A);
+  } else {
+    if (ncomp == 4) k_stokes<R, 2, 4><<<grid, kBlock, 0, st>>>(A);
+    else k_stokes<R, 2, 2><<<grid, kBlock, 0, st>>>(A);
+  }
+  return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_mask_copy(cx<R>* dst, const cx<R>* src, const Geo& g, int ncomp,
+                             cudaStream_t st) {
+  if (g.dim == 3) k_mask_copy<R, 3><<<grid_for(g.nspec), kBlock, 0, st>>>(dst, src, g, ncomp);
+  else k_mask_copy<R, 2><<<grid_for(g.nspec), kBlock, 0, st>>>(dst, src, g, ncomp);
+  return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_curl_masked(cx<R>* dst, const cx<R>* u, const Geo& g, cudaStream_t st) {
+  if (g.dim == 3) k_curl_masked<R, 3><<<grid_for(g.nspec), kBlock, 0, st>>>(dst, u, g);
+  else k_curl_masked<R, 2><<<grid_for(g.nspec), kBlock, 0, st>>>(dst, u, g);
+  return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_cross(R* u, const R* w, const Geo& g, unsigned long long* maxbits,
+                         cudaStream_t st) {
+  if (g.dim == 3) k_cross<R, 3><<<grid_for(g.nphys), kBlock, 0, st>>>(u, w, g, maxbits);
+  else k_cross<R, 2><<<grid_for(g.nphys), kBlock, 0, st>>>(u, w, g, maxbits);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_set_dt(double* dscal, const unsigned long long* maxbits, double cfl,
+                          cudaStream_t st) {
+  k_set_dt<<<1, 1, 0, st>>>(dscal, maxbits, cfl);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_advance_time(double* dscal, int n, cudaStream_t st) {
+  k_advance_time<<<1, 1, 0, st>>>(dscal, n);
+  return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_band_energy(const cx<R>* u, const Geo& g, double kf2, double* dscal,
+                               cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(dscal + kScalBandE, 0, sizeof(double), st);
+  if (e != cudaSuccess) return e;
+  if (g.dim == 3) k_band_energy<R, 3><<<grid_for(g.nspec), kBlock, 0, st>>>(u, g, kf2, dscal);
+  else k_band_energy<R, 2><<<grid_for(g.nspec), kBlock, 0, st>>>(u, g, kf2, dscal);
+  return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_energy(const cx<R>* u, const Geo& g, double* out2, cudaStream_t st) {
+  if (g.dim == 3) k_energy<R, 3><<<grid_for(g.nspec), kBlock, 0, st>>>(u, g, out2);
+  else k_energy<R, 2><<<grid_for(g.nspec), kBlock, 0, st>>>(u, g, out2);
+  return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_spectrum(const cx<R>* u, const Geo& g, double* out, int nbins,
+                            double kunit, cudaStream_t st) {
+  if (g.dim == 3) k_spectrum<R, 3><<<grid_for(g.nspec), kBlock, 0, st>>>(u, g, out, nbins, kunit);
+  else k_spectrum<R, 2><<<grid_for(g.nspec), kBlock, 0, st>>>(u, g, out, nbins, kunit);
+  return cudaGetLastError();
+}
+
+#define PF_INST(R)                                                                          \
+  template cudaError_t launch_update<R>(const UpdateArgs<R>&, int, cudaStream_t);           \
+  template cudaError_t launch_stokes<R>(const StokesArgs<R>&, int, cudaStream_t);           \
+  template cudaError_t launch_mask_copy<R>(cx<R>*, const cx<R>*, const Geo&, int,           \
+                                           cudaStream_t);                                   \
+  template cudaError_t launch_curl_masked<R>(cx<R>*, const cx<R>*, const Geo&,              \
+                                             cudaStream_t);                                 \
+  template cudaError_t launch_cross<R>(R*, const R*, const Geo&, unsigned long long*,       \
+                                       cudaStream_t);                                       \
+  template cudaError_t launch_band_energy<R>(const cx<R>*, const Geo&, double, double*,     \
+                                             cudaStream_t);                                 \
+  template cudaError_t launch_energy<R>(const cx<R>*, const Geo&, double*, cudaStream_t);   \
+  template cudaError_t launch_spectrum<R>(const cx<R>*, const Geo&, double*, int, double,   \
+                                          cudaStream_t);
+PF_INST(float)
+PF_INST(double)
+#undef PF_INST
+
+}  // namespace pf

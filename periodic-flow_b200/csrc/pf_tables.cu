@@ -1,0 +1,91 @@
+// Twiddle tables of the FFT engine, one static copy per device.
+#include <cmath>
+#include <mutex>
+#include <vector>
+
+#include "pf_fft.cuh"
+#include "pf_internal.h"
+
+namespace pf {
+
+static __device__ float2 g_tw_f32[kTwSize];
+static __device__ double2 g_tw_f64[kTwSize];
+
+// device addresses of the tables, per device
+static std::vector<const float2*> s_tw32;
+static std::vector<const double2*> s_tw64;
+
+// exp(-2 pi i m / n) in FP64, evaluated on the first octant and mapped by
+// symmetry so every entry is as accurate as the host sin/cos near zero.
+static void root_of_unity(long m, long n, double* c, double* s) {
+  // reduce m/n to [0, 1/8] and reflect
+  long a = (8 * m) / n;  // octant
+  double ang;
+  const double t = 2.0 * M_PI / (double)n;
+  long mm = m;
+  double cc, ss;
+  switch (a) {
+    case 0: ang = t * mm; cc = cos(ang); ss = sin(ang); break;
+    case 1: ang = t * ((double)n / 4 - mm); cc = sin(ang); ss = cos(ang); break;
+    case 2: ang = t * (mm - (double)n / 4); cc = -sin(ang); ss = cos(ang); break;
+    case 3: ang = t * ((double)n / 2 - mm); cc = -cos(ang); ss = sin(ang); break;
+    case 4: ang = t * (mm - (double)n / 2); cc = -cos(ang); ss = -sin(ang); break;
+    case 5: ang = t * (3.0 * n / 4 - mm); cc = -sin(ang); ss = -cos(ang); break;
+    case 6: ang = t * (mm - 3.0 * n / 4); cc = sin(ang); ss = -cos(ang); break;
+    default: ang = t * ((double)n - mm); cc = cos(ang); ss = -sin(ang); break;
+  }
+  *c = cc;
+  *s = -ss;  // exp(-i theta)
+}
+
+cudaError_t ensure_tables() {
+  static std::mutex mu;
+  static std::vector<int> done;  // per device
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)done.size() > dev && done[dev]) return cudaSuccess;
+  std::vector<float2> f(kTwSize);
+  std::vector<double2> d(kTwSize);
+  for (int n = 2; n <= kMaxFFT; n *= 2) {
+    for (int m = 0; m < n; ++m) {
+      double c, s;
+      root_of_unity(m, n, &c, &s);
+      d[n - 2 + m] = make_double2(c, s);
+      f[n - 2 + m] = make_float2((float)c, (float)s);
+    }
+  }
+  e = cudaMemcpyToSymbol(g_tw_f32, f.data(), sizeof(float2) * kTwSize);
+  if (e != cudaSuccess) return e;
+  e = cudaMemcpyToSymbol(g_tw_f64, d.data(), sizeof(double2) * kTwSize);
+  if (e != cudaSuccess) return e;
+  void* p32 = nullptr;
+  void* p64 = nullptr;
+  e = cudaGetSymbolAddress(&p32, g_tw_f32);
+  if (e != cudaSuccess) return e;
+  e = cudaGetSymbolAddress(&p64, g_tw_f64);
+  if (e != cudaSuccess) return e;
+  if ((int)done.size() <= dev) {
+    done.resize(dev + 1, 0);
+    s_tw32.resize(dev + 1, nullptr);
+    s_tw64.resize(dev + 1, nullptr);
+  }
+  s_tw32[dev] = (const float2*)p32;
+  s_tw64[dev] = (const double2*)p64;
+  done[dev] = 1;
+  return cudaSuccess;
+}
+
+template <> const float2* tw_base<float>() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev >= (int)s_tw32.size()) return nullptr;
+  return s_tw32[dev];
+}
+template <> const double2* tw_base<double>() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev >= (int)s_tw64.size()) return nullptr;
+  return s_tw64[dev];
+}
+
+}  // namespace pf

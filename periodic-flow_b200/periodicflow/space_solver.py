@@ -1,0 +1,222 @@
+"""Spatial operator of the solver (the reference's space_solver.py:67-310).
+
+The state lives on the GPU inside a C-ABI solver handle; ``u_hat`` and ``u``
+are host (NumPy, FP64) views materialised on access, and assignments upload.
+The right-hand side (nonlinear term, Leray projection, linear term, noise,
+forcing) is computed fused with the stage update on the device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from . import logger
+from .basis import FourierSpace
+
+NOISE_SOURCES = ("philox", "numpy", "injected")
+
+
+class SpaceSolver(FourierSpace):
+    def __init__(self, comm, mpi_rank, N_, is_nonlinear: bool = True, viscosity: float = 1e-3,
+                 noise_type: str = "thermal", noise_mag: float = 0.0, *, dt: float = 1e-3,
+                 integrator_id: int = N.PF_RK2, precision: str = "fp32", seed: int = 0,
+                 noise_source: str = "philox", forcing=None, cfl=None, fused: bool = True,
+                 **kwargs):
+        super().__init__(comm, mpi_rank, N_, **kwargs)
+        if self.dim not in (2, 3):
+            raise ValueError("NS solver only supports 2D and 3D problems.")
+        if noise_type not in ("thermal", "correlated"):
+            raise ValueError(f"Invalid noise type '{noise_type}'. Options are 'thermal' or 'correlated'.")
+        if noise_source not in NOISE_SOURCES:
+            raise ValueError(f"noise_source must be one of {NOISE_SOURCES}")
+        if precision not in ("fp32", "fp64"):
+            raise ValueError("precision must be 'fp32' or 'fp64'")
+        if is_nonlinear and self.dealias_rule == "pad":
+            raise NotImplementedError(
+                "dealias='3/2' (padding) is not built for the nonlinear term; use dealias='2/3'")
+        self._is_nonlinear = is_nonlinear
+        self.viscosity = viscosity
+        self.noise_type = noise_type
+        self.noise_mag = noise_mag
+        self.noise_source = noise_source
+        self.precision = precision
+        self.shape_local_physical = (self.dim,) + self.shape_physical
+        self.shape_local_fourier = (self.dim,) + self.shape_spectral
+        self.ncomp = self.dim ** 2 if noise_type == "thermal" else self.dim
+        # space_solver.py:143-148
+        self._k0_mask_0 = np.where(self.k2 == 0, 0, 1)
+        self._noise_normal_factor = self._k0_mask_0 / np.sqrt(np.prod(self.N)) / np.sqrt(
+            2 - 2 / self.dim)
+        self.linear_operator = -viscosity * self.k2
+        self.correlation_func = np.zeros(self.shape_spectral)
+        self.forcing_cfg = forcing
+        cfg = N.PfConfig()
+        N.lib().pf_config_default(C.byref(cfg))
+        cfg.dim = self.dim
+        for a in range(3):
+            cfg.n[a] = self.N[a] if a < self.dim else 1
+            lo, hi = self.domain[a] if a < self.dim else (0.0, 2 * np.pi)
+            cfg.domain[a][0] = lo
+            cfg.domain[a][1] = hi
+        cfg.is_nonlinear = int(bool(is_nonlinear))
+        cfg.integrator = integrator_id
+        cfg.viscosity = viscosity
+        cfg.noise_type = N.PF_NOISE_THERMAL if noise_type == "thermal" else N.PF_NOISE_CORRELATED
+        cfg.noise_mag = noise_mag
+        cfg.dealias = N.PF_DEALIAS_TRUNCATE
+        cfg.mask_nyquist = int(self.nyquist_mask is not None)
+        cfg.precision = N.PF_FP64 if precision == "fp64" else N.PF_FP32
+        cfg.dt = dt
+        cfg.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+        cfg.noise_source = N.PF_NOISE_SRC_PHILOX if noise_source == "philox" else N.PF_NOISE_SRC_INJECTED
+        if forcing is not None:
+            cfg.forcing_eps, cfg.forcing_kf = float(forcing[0]), float(forcing[1])
+        cfg.cfl = float(cfl) if cfl else 0.0
+        cfg.fused = int(bool(fused))
+        h = C.c_void_p()
+        N.check(N.lib().pf_create(C.byref(cfg), C.byref(h)), None, "pf_create")
+        self._h = h
+        self._cfg = cfg
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                N.lib().pf_destroy(h)
+            except Exception:  # pragma: no cover - interpreter shutdown
+                pass
+            self._h = None
+
+    # ------------------------------------------------------------ state views
+    @property
+    def u_hat(self) -> np.ndarray:
+        out = np.empty(self.shape_local_fourier, dtype=np.complex128)
+        N.check(N.lib().pf_get_fourier(self._h, out.ctypes.data, 0), self._h, "get u_hat")
+        return out
+
+    @u_hat.setter
+    def u_hat(self, value):
+        a = np.ascontiguousarray(np.broadcast_to(value, self.shape_local_fourier),
+                                 dtype=np.complex128)
+        N.check(N.lib().pf_set_fourier(self._h, a.ctypes.data, 0), self._h, "set u_hat")
+
+    @property
+    def u(self) -> np.ndarray:
+        """Physical velocity: backward transform of the current state."""
+        out = np.empty(self.shape_local_physical, dtype=np.float64)
+        N.check(N.lib().pf_get_physical(self._h, out.ctypes.data, 0), self._h, "get u")
+        return out
+
+    @u.setter
+    def u(self, value):
+        a = np.ascontiguousarray(np.broadcast_to(value, self.shape_local_physical),
+                                 dtype=np.float64)
+        N.check(N.lib().pf_set_physical(self._h, a.ctypes.data, 0), self._h, "set u")
+
+    # space_solver.py:180-213
+    def initialize_velocity(self, u0, space: str = "physical", mask_zero_mode: bool = True):
+        if space.casefold() == "physical":
+            if tuple(np.shape(u0)) != self.shape_local_physical:
+                raise ValueError(
+                    "SpaceSolver.initialize_velocity: Invalid shape for the input physical "
+                    f"velocity. Expected {self.shape_local_physical}, got {np.shape(u0)}.")
+            self.u = u0
+        elif space.casefold() == "fourier":
+            if tuple(np.shape(u0)) != self.shape_local_fourier:
+                raise ValueError(
+                    "SpaceSolver.initialize_velocity: Invalid shape for the input Fourier "
+                    f"velocity. Expected {self.shape_local_fourier}, got {np.shape(u0)}.")
+            self.u_hat = u0
+            if mask_zero_mode:
+                N.check(N.lib().pf_mask_zero_mode(self._h), self._h, "mask zero mode")
+        else:
+            raise ValueError("SpaceSolver.initialize_velocity: Invalid space type. Options are "
+                             "'physical' or 'fourier'.")
+
+    def project(self):
+        """Leray projection of the state in place (math.leray_projection on u_hat)."""
+        N.check(N.lib().pf_project(self._h), self._h, "project")
+
+    def forward(self, u=None):
+        """V.forward: physical -> spectral (space_solver.py:215-219)."""
+        if u is not None:
+            self.u = u
+
+    def backward(self):
+        """V.backward (space_solver.py:221-225): returns the physical field."""
+        return self.u
+
+    def set_linear_operator(self, L):
+        L = np.ascontiguousarray(np.broadcast_to(L, self.shape_spectral), dtype=np.float64)
+        self.linear_operator[...] = L
+        N.check(N.lib().pf_set_linear_operator(self._h, L.ctypes.data, 0), self._h,
+                "set_linear_operator")
+
+    def set_correlation_function(self, Cf):
+        Cf = np.ascontiguousarray(np.broadcast_to(np.real(Cf), self.shape_spectral),
+                                  dtype=np.float64)
+        self.correlation_func[...] = Cf
+        N.check(N.lib().pf_set_correlation(self._h, Cf.ctypes.data, 0), self._h,
+                "set_correlation_function")
+
+    # ---------------------------------------------------------------- noise
+    def random_fields(self):
+        """Draw w1, w2 for the next step with NumPy's global generator in the
+        reference's order (space_solver.py:227-238) and hand them to the device."""
+        shape = (self.ncomp,) + self.shape_spectral
+        w1 = np.random.randn(*shape) + 1j * np.random.randn(*shape)
+        w2 = np.random.randn(*shape) + 1j * np.random.randn(*shape)
+        w1 *= self._noise_normal_factor
+        w2 *= self._noise_normal_factor
+        self.inject_noise(w1, w2)
+        return w1, w2
+
+    def inject_noise(self, w1, w2):
+        shape = (self.ncomp,) + self.shape_spectral
+        a = np.ascontiguousarray(np.broadcast_to(w1, shape), dtype=np.complex128)
+        b = np.ascontiguousarray(np.broadcast_to(w2, shape), dtype=np.complex128)
+        N.check(N.lib().pf_inject_noise(self._h, a.ctypes.data, b.ctypes.data, 0), self._h,
+                "inject_noise")
+
+    def compute_rhs(self, a: float = 0.0):  # pragma: no cover - documented gap
+        raise NotImplementedError(
+            "the right-hand side is fused with the stage update on the device; use Solver.solve")
+
+    # ------------------------------------------------------------ diagnostics
+    def energy(self):
+        e, z = C.c_double(), C.c_double()
+        N.check(N.lib().pf_energy(self._h, C.byref(e), C.byref(z)), self._h, "energy")
+        return e.value, z.value
+
+    def spectrum(self, nbins: int | None = None):
+        if nbins is None:
+            nbins = int(np.sqrt(sum((n // 2) ** 2 for n in self.N))) + 2
+        out = np.zeros(nbins)
+        N.check(N.lib().pf_spectrum(self._h, out.ctypes.data, nbins), self._h, "spectrum")
+        return out
+
+    def step(self, nsteps: int):
+        N.check(N.lib().pf_step(self._h, int(nsteps)), self._h, "step")
+
+    def time(self):
+        t, s, dt = C.c_double(), C.c_longlong(), C.c_double()
+        N.check(N.lib().pf_get_time(self._h, C.byref(t), C.byref(s), C.byref(dt)), self._h, "time")
+        return t.value, s.value, dt.value
+
+    def set_time(self, t: float, step: int):
+        N.check(N.lib().pf_set_time(self._h, float(t), int(step)), self._h, "set_time")
+
+    def record_history(self, enable: bool = True):
+        N.check(N.lib().pf_record_history(self._h, int(bool(enable))), self._h, "record_history")
+
+    def history(self):
+        cap = 1 << 20
+        out = np.zeros((cap, 2))
+        cnt = C.c_int()
+        N.check(N.lib().pf_history(self._h, out.ctypes.data, cap, C.byref(cnt)), self._h, "history")
+        return out[:cnt.value].copy()
+
+
+__all__ = ["SpaceSolver", "logger"]

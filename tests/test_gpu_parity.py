@@ -1,0 +1,216 @@
+"""GPU parity of the CUDA path against the oracle and the golden fixtures.
+
+Tolerances (relative L2 over all modes of the state): FP64 1e-12 per the
+target (1e-11 where many FFT passes accumulate), FP32 1e-5.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-11, "fp32": 1e-5}
+
+
+def solver(N, dt=0.01, **kw):
+    from periodicflow import simulation as sim
+    kw.setdefault("dealias", "2/3")
+    return sim.Solver(list(N), dt, 1.0, **kw)
+
+
+# ------------------------------------------------------------------ transforms
+@pytest.mark.parametrize("N", [(8, 8), (32, 64), (256, 256), (1024, 16), (8, 8, 8),
+                               (16, 8, 32), (64, 64, 64), (128, 32, 256), (4, 1024, 8)])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_forward_backward_vs_oracle(N, precision):
+    rng = np.random.default_rng(1)
+    g = O.Grid(N)
+    s = solver(N, is_nonlinear=False, precision=precision)
+    u = rng.standard_normal((len(N),) + tuple(N))
+    s.space_solver.u = u
+    uh = s.space_solver.u_hat
+    ref = g.forward(u)
+    assert rel_l2(uh, ref) < (1e-13 if precision == "fp64" else 2e-6)
+    # backward of a Hermitian-consistent spectrum
+    s.space_solver.u_hat = ref
+    back = s.space_solver.u
+    assert rel_l2(back, u) < (1e-13 if precision == "fp64" else 2e-6)
+
+
+def test_backward_non_hermitian_planes_match_irfftn():
+    """C2R takes only the real part of the DC / Nyquist entries, like irfftn."""
+    rng = np.random.default_rng(2)
+    N = (16, 16, 16)
+    g = O.Grid(N)
+    uh = rng.standard_normal((3,) + g.spec_shape) + 1j * rng.standard_normal((3,) + g.spec_shape)
+    s = solver(N, is_nonlinear=False, precision="fp64")
+    s.space_solver.u_hat = uh
+    assert rel_l2(s.space_solver.u, g.backward(uh)) < 1e-13
+
+
+# ------------------------------------------------------------- golden pipelines
+def _run_pipeline(meta, golden, precision):
+    name = meta["name"]
+    pre = f"p_{name}_"
+    noisy = pre + "w1" in golden
+    s = solver(meta["N"], dt=meta["dt"], is_nonlinear=meta["nonlinear"],
+               time_integrator=meta["integ_name"], viscosity=meta["nu"],
+               noise_type=meta.get("noise_type", "thermal"), noise_mag=meta.get("noise_mag", 0.0),
+               domain=[(0.0, float(x)) for x in meta["L"]], mask_nyquist=meta["mask_nyquist"],
+               precision=precision, noise_source="injected" if noisy else "philox")
+    if meta["has_L"]:
+        s.set_linear_operator(golden[pre + "L"])
+    if meta["has_C"]:
+        s.set_correlation_function(golden[pre + "C"])
+    s.initialize(golden[pre + "uh0"], "fourier", project=False, mask_zero_mode=False)
+    states = golden[pre + "states"]
+    errs = []
+    for i in range(meta["nsteps"]):
+        if noisy:
+            s.inject_noise(golden[pre + "w1"][i], golden[pre + "w2"][i])
+        s.space_solver.step(1)
+        errs.append(rel_l2(s.space_solver.u_hat, states[i]))
+    return errs
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_golden_pipelines(golden, pipeline_meta, precision):
+    bad = {}
+    for name, meta in pipeline_meta.items():
+        errs = _run_pipeline(meta, golden, precision)
+        if max(errs) > TOL[precision]:
+            bad[name] = errs
+    assert not bad, bad
+
+
+# ------------------------------------------------------------------ operators
+@pytest.mark.parametrize("d,N", [(2, (8, 8)), (3, (8, 8, 8))])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_operator_kernels_vs_golden(golden, d, N, precision):
+    from periodicflow import math as pm
+    g = O.Grid(N)
+    cdt = np.complex128 if precision == "fp64" else np.complex64
+    rdt = np.float64 if precision == "fp64" else np.float32
+    tol = 1e-13 if precision == "fp64" else 1e-6
+    uh = golden[f"k{d}_uh"].astype(cdt)
+    k = g.k.astype(rdt)
+    c = np.zeros((3,) + g.spec_shape if d == 3 else g.spec_shape, dtype=cdt)
+    pm.curl(c, k, uh)
+    assert rel_l2(c, golden[f"k{d}_curl"]) < tol
+    u, w = golden[f"k{d}_u"].astype(rdt), golden[f"k{d}_w"].astype(rdt)
+    cr = np.zeros_like(u)
+    pm.cross(cr, u, w)
+    assert rel_l2(cr, golden[f"k{d}_cross"]) < tol
+    Lu = np.zeros_like(uh)
+    pm.apply_linear_operator(Lu, golden[f"k{d}_L"].astype(rdt), uh)
+    assert rel_l2(Lu, golden[f"k{d}_Lu"]) < tol
+    up = uh.copy()
+    p = np.zeros(g.spec_shape, dtype=cdt)
+    pm.leray_projection(up, k, g.k_over_k2.astype(rdt), p)
+    assert rel_l2(up, golden[f"k{d}_leray_u"]) < tol
+    assert rel_l2(p, golden[f"k{d}_leray_p"]) < tol
+    W = golden[f"k{d}_W"].astype(cdt)
+    ws = np.zeros_like(W)
+    pm.symmetrize(ws, W)
+    assert rel_l2(ws, golden[f"k{d}_Wsym"]) < tol
+    div = np.zeros((d,) + g.spec_shape, dtype=cdt)
+    pm.noise_divergence(div, ws, k)
+    assert rel_l2(div, golden[f"k{d}_noisediv"]) < tol
+
+
+@pytest.mark.parametrize("d", [2, 3])
+@pytest.mark.parametrize("name", ["explicit_pc", "implicit_pc", "rk2", "rk3", "rk4"])
+def test_stepping_kernels_vs_golden(golden, d, name):
+    from periodicflow.time_integrator import DICT_TIME_INTEGRATORS
+    L = golden[f"st{d}_L"]
+    integ = DICT_TIME_INTEGRATORS[name](0.01, L.copy())
+    for stage in range(integ.n_stages):
+        key = f"st{d}_{name}_1_{stage}"
+        unew, u0, Nl, Lu, f, xi = (a.copy() for a in golden[key + "_in"])
+        integ.stepping(unew, u0, stage, Nl, Lu, f, xi)
+        assert rel_l2(unew, golden[key + "_out"]) < 1e-14
+        assert rel_l2(Lu, golden[key + "_Lu"]) < 1e-14
+
+
+# ---------------------------------------------------------------- Philox noise
+@pytest.mark.parametrize("N,noise_type,integ", [
+    ((16, 16), "thermal", "explicit_pc"), ((16, 16), "thermal", "implicit_pc"),
+    ((16, 16), "correlated", "implicit_pc"), ((8, 8, 8), "thermal", "rk3"),
+    ((8, 8, 8), "correlated", "explicit_pc")])
+def test_philox_stokes_vs_oracle(N, noise_type, integ):
+    """Device Philox draws (Hermitian on self-conjugate planes) == oracle's."""
+    nu, mag = 0.1, 0.05
+    g = O.Grid(N)
+    Cf = np.exp(-g.k2 / 8.0) * g.mask_k0
+    o = O.OracleSolver(N, 0.01, is_nonlinear=False, time_integrator=integ, viscosity=nu,
+                       noise_type=noise_type, noise_mag=mag, noise="philox", seed=1234)
+    s = solver(N, is_nonlinear=False, time_integrator=integ, viscosity=nu,
+               noise_type=noise_type, noise_mag=mag, precision="fp64", seed=1234)
+    if noise_type == "correlated":
+        o.set_correlation_function(Cf)
+        s.set_correlation_function(Cf)
+    s.space_solver.step(3)
+    o.advance(3)
+    assert rel_l2(s.space_solver.u_hat, o.u_hat) < 1e-12
+
+
+def test_philox_nonlinear_noise_generic_update_vs_oracle():
+    N = (32, 32)
+    o = O.OracleSolver(N, 0.01, time_integrator="rk3", viscosity=0.01, noise_mag=0.05,
+                       noise="philox", seed=99)
+    s = solver(N, time_integrator="rk3", viscosity=0.01, noise_mag=0.05, precision="fp64",
+               seed=99)
+    uh0 = O.spectral_random_field(o.grid, 3, kp=3.0)
+    o.initialize(uh0, "fourier")
+    s.initialize(uh0, "fourier")
+    s.space_solver.step(3)
+    o.advance(3)
+    assert rel_l2(s.space_solver.u_hat, o.u_hat) < 1e-11
+
+
+def test_stokes_multistep_kernel_equals_single_steps():
+    N = (32, 32)
+    kw = dict(is_nonlinear=False, time_integrator="explicit_pc", viscosity=0.1,
+              noise_mag=0.01, precision="fp32", seed=5)
+    a = solver(N, **kw)
+    b = solver(N, **kw)
+    a.space_solver.step(10)
+    for _ in range(10):
+        b.space_solver.step(1)
+    np.testing.assert_array_equal(a.space_solver.u_hat, b.space_solver.u_hat)
+
+
+# ---------------------------------------------------------- TGV / forcing / CFL
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_tgv64_rk4_energy_enstrophy(precision):
+    """Taylor-Green 64^3, nu=1/1600, rk4, dt=0.005: E, Z per step vs oracle."""
+    N = (64, 64, 64)
+    o = O.OracleSolver(N, 0.005, time_integrator="rk4", viscosity=1 / 1600)
+    o.initialize(O.taylor_green(o.grid))
+    s = solver(N, dt=0.005, time_integrator="rk4", viscosity=1 / 1600, precision=precision,
+               diagnostics=True)
+    s.initialize(O.taylor_green(o.grid))
+    hist_o = o.advance(10, diagnostics=True)
+    s.space_solver.step(10)
+    hist_s = s.space_solver.history()
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    assert rel_l2(s.space_solver.u_hat, o.u_hat) < tol * 10
+    assert np.max(np.abs(hist_s - np.array(hist_o)) / np.abs(np.array(hist_o))) < tol
+
+
+def test_forcing_and_cfl_rk3_vs_oracle():
+    N = (32, 32, 32)
+    o = O.OracleSolver(N, 0.01, time_integrator="rk3", viscosity=2e-3, forcing=(0.1, 2.5),
+                       cfl=0.5)
+    uh0 = O.spectral_random_field(o.grid, 1)
+    o.initialize(uh0, "fourier")
+    s = solver(N, time_integrator="rk3", viscosity=2e-3, forcing=(0.1, 2.5), cfl=0.5,
+               precision="fp64")
+    s.initialize(uh0, "fourier")
+    o.advance(4)
+    s.space_solver.step(4)
+    t, step, dt = s.space_solver.time()
+    assert step == 4 and abs(t - o.t) < 1e-12 * o.t and abs(dt - o.dt) < 1e-12 * o.dt
+    assert rel_l2(s.space_solver.u_hat, o.u_hat) < 1e-11
