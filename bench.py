@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Benchmark of the periodicflow B200 backend.
+
+Workload (N=1): 3D forced isotropic turbulence on a 256^3 box, FP32, TVD RK3
+with CFL 0.5, linear band forcing (|k| <= 2.5, eps = 0.1), nu = 2e-3, 2/3
+dealiasing, random solenoidal initial field E(k) ~ k^4 exp(-2 (k/4)^2) (seed 1),
+synthetic (no dataset is involved).  One step = one full RK3 time step (three
+stages) on the device.  Metric: Mpts * RK-steps / s = 256^3 / 1e6 * steps / s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank advances its own
+independent box (seed 1 + rank): weak scaling, no data-path collective; the
+time is the max over ranks.  ``--impl reference`` times the CPU oracle (the
+FP64 NumPy/SciPy restatement of the reference's path) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "periodic-flow_b200"))
+
+METRIC = "Mpts*RK-steps/s at 256^3 FP32"
+UNIT = "Mpts*steps/s"
+
+CFG = dict(n=256, nu=2e-3, integrator="rk3", cfl=0.5, forcing=(0.1, 2.5), seed=1, dt0=1e-3)
+
+# Algorithmic bytes per launch of each timed pass, in units of one FP32 complex
+# half-spectrum field U = n0 n1 (n2/2+1) 8 B, for the 2/3-rule fused schedule
+# (c = 2 kmax + 1 kept indices of a complex axis, c2 = kmax + 1 of the last one).
+
+
+def pass_bytes(n):
+    nh = n // 2 + 1
+    kmax = (n - 1) // 3
+    c1, c2 = 2 * kmax + 1, kmax + 1
+    cb = 8
+    U = n * n * nh * cb
+    return {
+        "P1": (3 * c1 * c1 * c2 + 5 * n * c1 * c2) * cb,
+        "P2": (5 * n * c1 * c2 + 6 * n * n * c2) * cb,
+        "P3": (6 * n * n * c2) * cb + 3 * U,
+        "P4": 6 * U,
+        "P5": 12 * U,  # nl (3) + u_hat (3) + u0 (3) read, u_hat (3) written
+        "U": U,
+    }
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        lr = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(lr)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", lr))
+        return dist, dist.get_rank(), ws
+    return None, 0, 1
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return float("nan")
+        sm = np.array([num(r[1]) for r in rows])
+        smax = np.array([num(r[2]) for r in rows])
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.nanmedian(sm)), "sm_max_mhz": float(np.nanmax(smax)),
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": float(np.nanmax([num(r[3]) for r in rows]))}
+
+
+def initial_field(n, seed):
+    """Product-side initial field (host NumPy set-up)."""
+    from periodicflow import _comm
+    from periodicflow.basis import FourierSpace
+    from periodicflow.initial import spectral_random_field
+    return spectral_random_field(FourierSpace(_comm.COMM_WORLD, 0, [n] * 3, dealias="2/3"), seed)
+
+
+def oracle_initial_field(n, seed):
+    import oracle as O
+    return O.spectral_random_field(O.Grid((n, n, n)), seed)
+
+
+def make_solver(n, precision="fp32"):
+    from periodicflow import simulation as sim
+    return sim.Solver([n] * 3, CFG["dt0"], 1.0, time_integrator=CFG["integrator"],
+                      viscosity=CFG["nu"], dealias="2/3", precision=precision,
+                      forcing=CFG["forcing"], cfl=CFG["cfl"])
+
+
+def run_ours(args, dist, rank, world):
+    import torch
+    from periodicflow import _native as N
+    import ctypes as C
+    n = args.n
+    dev = torch.cuda.current_device()
+    uh0 = initial_field(n, CFG["seed"] + rank)
+    sol = make_solver(n)
+    ss = sol.space_solver
+    ss.initialize_velocity(uh0, "fourier")
+    ss.step(args.warmup)
+    torch.cuda.synchronize()
+    lib = N.lib()
+    # ------------------------------------------------------------ timed region
+    dominant = N.PF_PASS_FUSED[args.timed_pass]
+    N.check(lib.pf_kernel_timer(ss._h, dominant), ss._h, "timer")
+    c0 = C.c_longlong()
+    lib.pf_launch_count(C.byref(c0))
+    clocks = ClockSampler(dev)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    ss.step(args.steps)
+    ev1.record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ck = clocks.stop()
+    c1 = C.c_longlong()
+    lib.pf_launch_count(C.byref(c1))
+    ms = ev0.elapsed_time(ev1)
+    tot_ms, nl = C.c_double(), C.c_longlong()
+    N.check(lib.pf_kernel_timer_read(ss._h, C.byref(tot_ms), C.byref(nl)), ss._h, "timer")
+    lib.pf_kernel_timer(ss._h, -1)
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    pts = n ** 3 / 1e6
+    value = world * pts * args.steps / (ms / 1e3)
+    _, _, dt_now = ss.time()
+    # ---------------------------------------------------------------- roofline
+    pb = pass_bytes(n)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    avg_s = tot_ms.value / max(nl.value, 1) / 1e3
+    alg = pb[f"P{args.timed_pass}"]
+    achieved = alg / avg_s / 1e9 if avg_s > 0 else None
+    roofline = {"bound": "hbm", "kernel": f"fused pass P{args.timed_pass}",
+                "achieved": achieved, "peak": peak, "peak_source": peak_src, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None,
+                "traffic": args.traffic, "alg_bytes_per_launch": alg,
+                "avg_launch_ms": avg_s * 1e3, "launches_timed": nl.value}
+    step_bytes = 3 * sum(pb[f"P{i}"] for i in range(1, 6))
+    step_roof = {"alg_bytes_per_step": step_bytes,
+                 "achieved_gbs": step_bytes / (ms / args.steps / 1e3) / 1e9 * 1.0,
+                 "frac": step_bytes / (ms / args.steps / 1e3) / 1e9 / peak}
+    # --------------------------------------------------------------------- e2e
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, uh0, rank, dist)
+    # ------------------------------------------------------------ cpu baseline
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(n, args.cpu_steps)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": f"3D forced isotropic turbulence {n}^3, RK3 CFL 0.5, "
+                                   "linear forcing |k|<=2.5 eps=0.1, nu=2e-3, 2/3 dealias",
+                       "grid": [n, n, n], "integrator": "rk3", "replicas_per_gpu": 1,
+                       "parallelism": f"replicas x{world} (one box per GPU)",
+                       "l2": "working set > L2 (state 3x67.6 MB + intermediates)",
+                       "dt_after_run": dt_now},
+            "gpu_launches": int(c1.value - c0.value),
+            "clocks": ck, "roofline": roofline, "step_roofline": step_roof,
+            "e2e": e2e, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def run_e2e(args, uh0, rank, dist):
+    """Same metric through the public API with host buffers: upload the state
+    from pinned host memory, then per step one step and an E, Z read-back,
+    then download the final state; copies inside the timed region."""
+    import torch
+    n = args.n
+    pinned = torch.empty(uh0.shape, dtype=torch.complex128, pin_memory=True)
+    pinned.numpy()[...] = uh0
+    host_in = pinned.numpy()
+    out_pinned = torch.empty(uh0.shape, dtype=torch.complex128, pin_memory=True)
+    sol = make_solver(n)
+    ss = sol.space_solver
+    ss.initialize_velocity(host_in, "fourier")
+    ss.step(args.warmup)
+    torch.cuda.synchronize()
+    import ctypes as C
+    from periodicflow import _native as N
+    K = args.e2e_steps
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    ss.initialize_velocity(host_in, "fourier")
+    ez = []
+    for _ in range(K):
+        ss.step(1)
+        ez.append(ss.energy())
+    N.check(N.lib().pf_get_fourier(ss._h, C.c_void_p(out_pinned.data_ptr()), 0), ss._h, "get")
+    t1 = time.perf_counter()
+    sec = t1 - t0
+    if dist:
+        t = torch.tensor([sec], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sec = float(t.item())
+    world = dist.get_world_size() if dist else 1
+    state_b = int(np.prod(uh0.shape)) * 16
+    return {"value": world * n ** 3 / 1e6 * K / sec, "unit": UNIT, "steps": K,
+            "h2d_bytes_per_step": state_b / K, "d2h_bytes_per_step": (state_b + 16 * K) / K,
+            "note": "per step: pf_step(1) + E,Z read-back (16 B); state up/download "
+                    "(complex128) amortised over the steps; wall clock"}
+
+
+def cpu_baseline(n, steps):
+    """The oracle (FP64 NumPy + scipy.fft on all host cores) on the same box."""
+    import scipy.fft  # noqa: F401
+    import oracle as O
+    import oracle.pf_oracle as P
+    P.FFT_WORKERS = os.cpu_count()
+    o = O.OracleSolver((n, n, n), CFG["dt0"], time_integrator=CFG["integrator"],
+                       viscosity=CFG["nu"], forcing=CFG["forcing"], cfl=CFG["cfl"])
+    o.initialize(oracle_initial_field(n, CFG["seed"]), "fourier")
+    t0 = time.perf_counter()
+    o.advance(steps)
+    sec = time.perf_counter() - t0
+    return {"value": n ** 3 / 1e6 * steps / sec, "unit": UNIT, "cores": os.cpu_count(),
+            "kind": "port", "sample": f"{steps} full RK3 steps of the {n}^3 workload, FP64 "
+            f"oracle (NumPy pointwise single-threaded, scipy.fft workers={os.cpu_count()}), "
+            f"{sec:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    n = args.n
+    import oracle as O
+    import oracle.pf_oracle as P
+    P.FFT_WORKERS = os.cpu_count()
+    o = O.OracleSolver((n, n, n), CFG["dt0"], time_integrator=CFG["integrator"],
+                       viscosity=CFG["nu"], forcing=CFG["forcing"], cfl=CFG["cfl"])
+    o.initialize(oracle_initial_field(n, CFG["seed"]), "fourier")
+    warm = min(args.warmup, 1)
+    o.advance(warm)
+    budget = args.ref_budget_s
+    t0 = time.perf_counter()
+    done = 0
+    while done < args.steps:
+        o.advance(1)
+        done += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    sec = time.perf_counter() - t0
+    value = n ** 3 / 1e6 * done / sec
+    sample = (f"{done} of {args.steps} requested full RK3 steps (time box {budget:.0f} s) of the "
+              f"{n}^3 workload after {warm} warm-up step(s); FP64 oracle (NumPy + scipy.fft, "
+              f"{os.cpu_count()} workers)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": done, "warmup": warm, "ms_per_step": sec / done * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
+            "data": "synthetic",
+            "config": {"workload": f"3D forced isotropic turbulence {n}^3, RK3 CFL 0.5, "
+                                   "linear forcing |k|<=2.5 eps=0.1, nu=2e-3, 2/3 dealias",
+                       "grid": [n, n, n]},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(),
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--timed-pass", type=int, default=5, choices=[1, 2, 3, 4, 5])
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="DRAM bytes per launch of the timed pass from an ncu capture")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--ref-budget-s", type=float, default=120.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference(args, rank, world)
+        return
+    dist, rank, world = _dist()
+    try:
+        run_ours(args, dist, rank, world)
+    finally:
+        if dist:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

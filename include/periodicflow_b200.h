@@ -138,6 +138,25 @@ int pf_record_history(pf_solver* h, int enable);
 /* Shell spectrum E(k), nbins bins of width 2 pi / L0. */
 int pf_spectrum(pf_solver* h, double* out, int nbins);
 
+/* ---- measurement ------------------------------------------------------- */
+/* kernel passes that can be timed */
+#define PF_PASS_UPDATE 0        /* fused stage update (Leray, L, noise, forcing) */
+#define PF_PASS_FFT_STRIDED 1   /* complex FFT along a strided axis */
+#define PF_PASS_FFT_LAST 2      /* C2R / R2C along the contiguous axis */
+#define PF_PASS_STOKES 4        /* whole steps of the linear problem */
+#define PF_PASS_FUSED_P1 11     /* fused nonlinear passes P1..P5 */
+#define PF_PASS_FUSED_P2 12
+#define PF_PASS_FUSED_P3 13
+#define PF_PASS_FUSED_P4 14
+#define PF_PASS_FUSED_P5 15
+/* Time every launch of `pass` with CUDA events on the handle's stream
+ * (-1 disables); accumulators restart. */
+int pf_kernel_timer(pf_solver* h, int pass);
+/* Sum of the timed launch durations (ms) and their count since the last read. */
+int pf_kernel_timer_read(pf_solver* h, double* total_ms, long long* launches);
+/* Total kernels launched by this library in this process. */
+int pf_launch_count(long long* count);
+
 /* ---- operators on device arrays (math.py / space_solver.py kernels) ------
  * Arrays are device pointers of element type double (PF_FP64) or float
  * (PF_FP32); complex arrays interleaved.  shape = spatial extents of one

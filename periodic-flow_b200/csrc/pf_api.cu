@@ -39,8 +39,24 @@ struct pf_solver {
   long long step = 0;
   double t = 0.0;
   FusedPlan* fused = nullptr;
+  // per-pass CUDA-event timing (pf_kernel_timer)
+  int tpass = -1;
+  std::vector<cudaEvent_t> tev;
+  size_t tused = 0;
   std::string err;
 };
+
+// record an event on the solver stream when `pass` is the timed pass; events
+// come in (begin, end) pairs around each launch of that pass
+static void tmark(pf_solver* h, int pass) {
+  if (h->tpass != pass) return;
+  if (h->tused == h->tev.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    h->tev.push_back(e);
+  }
+  cudaEventRecord(h->tev[h->tused++], h->st);
+}
 
 static const int kHist = 4096;
 static std::string g_static_err;
@@ -110,15 +126,27 @@ static cudaError_t backward_inplace(pf_solver* h, cx<R>* X, R* P, int nc) {
   cudaError_t e;
   if (g.dim == 3) {
     const long long plane = (long long)g.s[1] * g.nh;
+    tmark(h, PF_PASS_FFT_STRIDED);
     e = fft_strided<R>(X, g.n[0], +1, plane, nc, g.nspec, plane, 1.0, h->st);
+    tmark(h, PF_PASS_FFT_STRIDED);
     if (e != cudaSuccess) return e;
+    tmark(h, PF_PASS_FFT_STRIDED);
     e = fft_strided<R>(X, g.n[1], +1, g.nh, (long long)nc * g.n[0], plane, g.nh, 1.0, h->st);
+    tmark(h, PF_PASS_FFT_STRIDED);
     if (e != cudaSuccess) return e;
-    return fft_c2r_last<R>(X, P, g.n[2], (long long)nc * g.n[0] * g.n[1], g.nh, g.n[2], h->st);
+    tmark(h, PF_PASS_FFT_LAST);
+    e = fft_c2r_last<R>(X, P, g.n[2], (long long)nc * g.n[0] * g.n[1], g.nh, g.n[2], h->st);
+    tmark(h, PF_PASS_FFT_LAST);
+    return e;
   }
+  tmark(h, PF_PASS_FFT_STRIDED);
   e = fft_strided<R>(X, g.n[0], +1, g.nh, nc, g.nspec, g.nh, 1.0, h->st);
+  tmark(h, PF_PASS_FFT_STRIDED);
   if (e != cudaSuccess) return e;
-  return fft_c2r_last<R>(X, P, g.n[1], (long long)nc * g.n[0], g.nh, g.n[1], h->st);
+  tmark(h, PF_PASS_FFT_LAST);
+  e = fft_c2r_last<R>(X, P, g.n[1], (long long)nc * g.n[0], g.nh, g.n[1], h->st);
+  tmark(h, PF_PASS_FFT_LAST);
+  return e;
 }
 
 template <typename R>
@@ -128,15 +156,27 @@ static cudaError_t forward_into(pf_solver* h, const R* P, cx<R>* X, int nc) {
   cudaError_t e;
   if (g.dim == 3) {
     const long long plane = (long long)g.s[1] * g.nh;
+    tmark(h, PF_PASS_FFT_LAST);
     e = fft_r2c_last<R>(P, X, g.n[2], (long long)nc * g.n[0] * g.n[1], g.n[2], g.nh, scale, h->st);
+    tmark(h, PF_PASS_FFT_LAST);
     if (e != cudaSuccess) return e;
+    tmark(h, PF_PASS_FFT_STRIDED);
     e = fft_strided<R>(X, g.n[1], -1, g.nh, (long long)nc * g.n[0], plane, g.nh, 1.0, h->st);
+    tmark(h, PF_PASS_FFT_STRIDED);
     if (e != cudaSuccess) return e;
-    return fft_strided<R>(X, g.n[0], -1, plane, nc, g.nspec, plane, 1.0, h->st);
+    tmark(h, PF_PASS_FFT_STRIDED);
+    e = fft_strided<R>(X, g.n[0], -1, plane, nc, g.nspec, plane, 1.0, h->st);
+    tmark(h, PF_PASS_FFT_STRIDED);
+    return e;
   }
+  tmark(h, PF_PASS_FFT_LAST);
   e = fft_r2c_last<R>(P, X, g.n[1], (long long)nc * g.n[0], g.n[1], g.nh, scale, h->st);
+  tmark(h, PF_PASS_FFT_LAST);
   if (e != cudaSuccess) return e;
-  return fft_strided<R>(X, g.n[0], -1, g.nh, nc, g.nspec, g.nh, 1.0, h->st);
+  tmark(h, PF_PASS_FFT_STRIDED);
+  e = fft_strided<R>(X, g.n[0], -1, g.nh, nc, g.nspec, g.nh, 1.0, h->st);
+  tmark(h, PF_PASS_FFT_STRIDED);
+  return e;
 }
 
 // nonlinear term u x w (unprojected) of the current state into h->nl
@@ -225,11 +265,19 @@ static int step_generic(pf_solver* h) {
   const Scheme sc = make_scheme(h->cfg.integrator);
   const bool cfl = h->cfg.cfl > 0.0;
   const bool forcing = h->cfg.forcing_eps > 0.0;
+  const bool use_fused = h->fused != nullptr && h->cfg.fused && h->cfg.is_nonlinear;
   for (int s = 0; s < sc.nstages; ++s) {
     if (h->cfg.is_nonlinear) {
-      if (h->fused && h->cfg.fused) {
-        PF_CUDA(h, fused_nonlinear(h->fused, h->uhat, h->nl, (s == 0 && cfl) ? h->maxbits : nullptr,
-                                   h->st));
+      if (use_fused) {
+        if (s == 0 && cfl)
+          PF_CUDA(h, cudaMemsetAsync(h->maxbits, 0, sizeof(unsigned long long), h->st));
+        for (int p = 1; p <= 4; ++p) {
+          tmark(h, PF_PASS_FUSED_P1 + p - 1);
+          cudaError_t fe = fused_pass(h->fused, p, h->uhat, h->nl,
+                                      (s == 0 && cfl && p == 3) ? h->maxbits : nullptr, h->st);
+          tmark(h, PF_PASS_FUSED_P1 + p - 1);
+          PF_CUDA(h, fe);
+        }
       } else {
         PF_CUDA(h, nonlinear_generic<R>(h, s == 0 && cfl));
       }
@@ -264,7 +312,18 @@ static int step_generic(pf_solver* h) {
     A.save_u0 = s == 0;
     A.nyq_mask = h->cfg.mask_nyquist;
     A.forcing = forcing;
-    PF_CUDA(h, launch_update<R>(A, h->ncomp, h->st));
+    cudaError_t ue;
+    if (use_fused) {
+      tmark(h, PF_PASS_FUSED_P5);
+      if constexpr (sizeof(R) == 4) ue = fused_update(h->fused, A, h->ncomp, h->nl, h->st);
+      else ue = cudaErrorNotSupported;
+      tmark(h, PF_PASS_FUSED_P5);
+    } else {
+      tmark(h, PF_PASS_UPDATE);
+      ue = launch_update<R>(A, h->ncomp, h->st);
+      tmark(h, PF_PASS_UPDATE);
+    }
+    PF_CUDA(h, ue);
   }
   if (!cfl) PF_CUDA(h, launch_advance_time(h->dscal, 1, h->st));
   return PF_OK;
@@ -289,8 +348,22 @@ static int step_stokes(pf_solver* h, int nsteps) {
   A.nsteps = nsteps;
   A.noise_src = noise_src(h);
   A.noise_type = h->cfg.noise_type;
-  PF_CUDA(h, launch_stokes<R>(A, h->ncomp, h->st));
+  tmark(h, PF_PASS_STOKES);
+  cudaError_t se = launch_stokes<R>(A, h->ncomp, h->st);
+  tmark(h, PF_PASS_STOKES);
+  PF_CUDA(h, se);
   PF_CUDA(h, launch_advance_time(h->dscal, nsteps, h->st));
+  return PF_OK;
+}
+
+// Error word of bounded waits inside the fused passes (synchronous read).
+static int check_dev_errors(pf_solver* h) {
+  if (!h->fused) return PF_OK;
+  const int v = fused_device_error(h->fused);
+  if (v != 0)
+    return fail(h, PF_ERR_CUDA,
+                "a bounded device wait gave up (code " + std::to_string(v) +
+                    "): a bulk copy did not complete in time; results of the step are invalid");
   return PF_OK;
 }
 
@@ -466,6 +539,7 @@ int pf_destroy(pf_solver* h) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->fused) fused_destroy(h->fused);
+  for (cudaEvent_t e : h->tev) cudaEventDestroy(e);
   delete h;
   return PF_OK;
 }
@@ -500,13 +574,13 @@ static cudaError_t convert_in(pf_solver* h, void* dst, size_t n) {
   if (h->prec == PF_FP64)
     return cudaMemcpyAsync(dst, h->stage64, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->st);
   k_from64<float><<<blocks_for(n), 256, 0, h->st>>>((float*)dst, h->stage64, (long long)n);
-  return cudaGetLastError();
+  return launched();
 }
 static cudaError_t convert_out(pf_solver* h, const void* src, size_t n) {
   if (h->prec == PF_FP64)
     return cudaMemcpyAsync(h->stage64, src, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->st);
   k_to64<float><<<blocks_for(n), 256, 0, h->st>>>(h->stage64, (const float*)src, (long long)n);
-  return cudaGetLastError();
+  return launched();
 }
 
 int pf_set_fourier(pf_solver* h, const double* u_hat, int where) {
@@ -523,7 +597,8 @@ int pf_get_fourier(pf_solver* h, double* u_hat, int where) {
   if (!h || !u_hat) return fail(h, PF_ERR_INVALID, "pf_get_fourier: null argument");
   const size_t n = 2 * (size_t)h->d * h->g.nspec;
   PF_CUDA(h, convert_out(h, h->uhat, n));
-  return stage_out(h, u_hat, n, where);
+  int rc = stage_out(h, u_hat, n, where);
+  return rc ? rc : check_dev_errors(h);
 }
 
 int pf_set_physical(pf_solver* h, const double* u, int where) {
@@ -576,7 +651,7 @@ int pf_mask_zero_mode(pf_solver* h) {
   if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
   if (h->prec == PF_FP64) k_scale_mask0<double><<<1, 32, 0, h->st>>>((double2*)h->uhat, h->g, h->d);
   else k_scale_mask0<float><<<1, 32, 0, h->st>>>((float2*)h->uhat, h->g, h->d);
-  PF_CUDA(h, cudaGetLastError());
+  PF_CUDA(h, launched());
   return PF_OK;
 }
 
@@ -590,7 +665,7 @@ int pf_project(pf_solver* h) {
     if (h->d == 3) k_project<float, 3><<<b, 256, 0, h->st>>>((float2*)h->uhat, h->g);
     else k_project<float, 2><<<b, 256, 0, h->st>>>((float2*)h->uhat, h->g);
   }
-  PF_CUDA(h, cudaGetLastError());
+  PF_CUDA(h, launched());
   return PF_OK;
 }
 
@@ -651,7 +726,7 @@ int pf_get_time(pf_solver* h, double* t, long long* step, double* dt) {
   if (t) *t = sc[kScalTime];
   if (step) *step = h->step;
   if (dt) *dt = sc[kScalDt];
-  return PF_OK;
+  return check_dev_errors(h);
 }
 
 int pf_set_time(pf_solver* h, double t, long long step) {
@@ -675,7 +750,7 @@ int pf_energy(pf_solver* h, double* energy, double* enstrophy) {
   PF_CUDA(h, cudaStreamSynchronize(h->st));
   if (energy) *energy = r[0];
   if (enstrophy) *enstrophy = r[1];
-  return PF_OK;
+  return check_dev_errors(h);
 }
 
 int pf_record_history(pf_solver* h, int enable) {
@@ -710,6 +785,36 @@ int pf_spectrum(pf_solver* h, double* out, int nbins) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
   cudaFree(tmp);
   if (e != cudaSuccess) return fail(h, PF_ERR_CUDA, std::string("pf_spectrum: ") + cudaGetErrorString(e));
+  return PF_OK;
+}
+
+int pf_kernel_timer(pf_solver* h, int pass) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  h->tpass = pass;
+  h->tused = 0;
+  return PF_OK;
+}
+
+int pf_kernel_timer_read(pf_solver* h, double* total_ms, long long* launches) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  PF_CUDA(h, cudaStreamSynchronize(h->st));
+  double tot = 0.0;
+  long long n = 0;
+  for (size_t i = 0; i + 1 < h->tused; i += 2) {
+    float ms = 0.f;
+    PF_CUDA(h, cudaEventElapsedTime(&ms, h->tev[i], h->tev[i + 1]));
+    tot += ms;
+    ++n;
+  }
+  if (total_ms) *total_ms = tot;
+  if (launches) *launches = n;
+  h->tused = 0;
+  return PF_OK;
+}
+
+int pf_launch_count(long long* count) {
+  if (!count) return fail(nullptr, PF_ERR_INVALID, "null pointer");
+  *count = launch_total();
   return PF_OK;
 }
 

@@ -176,7 +176,7 @@ static cudaError_t launch_strided(cx<R>* data, int dir, long long ncols, long lo
     if (e != cudaSuccess) return e;
     k_fft_strided<R, N, +1><<<grid, block, sm, st>>>(data, ncols, ntotal, ps, ls, (R)scale, us, tw);
   }
-  return cudaGetLastError();
+  return launched();
 }
 
 template <typename R, int N>
@@ -194,7 +194,7 @@ static cudaError_t launch_c2r(const cx<R>* in, R* out, long long nlines, long lo
   cudaError_t e = set_smem(k_c2r_last<R, N>, sm);
   if (e != cudaSuccess) return e;
   k_c2r_last<R, N><<<grid, block, sm, st>>>(in, out, nlines, is, os, tw);
-  return cudaGetLastError();
+  return launched();
 }
 
 template <typename R, int N>
@@ -212,7 +212,7 @@ static cudaError_t launch_r2c(const R* in, cx<R>* out, long long nlines, long lo
   cudaError_t e = set_smem(k_r2c_last<R, N>, sm);
   if (e != cudaSuccess) return e;
   k_r2c_last<R, N><<<grid, block, sm, st>>>(in, out, nlines, is, os, (R)scale, tw);
-  return cudaGetLastError();
+  return launched();
 }
 
 bool fft_length_supported(int n) {

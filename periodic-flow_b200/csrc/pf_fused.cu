@@ -1,17 +1,660 @@
-// Fused pencil passes of the nonlinear term.
+// Fused pencil passes of the 3D nonlinear term with the 2/3 rule.
+//
+// Only modes with |k_i| <= kmax_i = (n_i - 1) / 3 feed u and omega, so the
+// inverse passes work on compact "kept" index ranges:  along a complex axis
+// the kept indices are [0, kmax] and [n - kmax, n), compacted to [0, c) with
+// c = 2 kmax + 1; along the last axis they are [0, kmax2], c2 = kmax2 + 1.
+//
+//   P1  inverse FFT along axis 0 of the kept (k1, k2) columns of u_hat
+//       -> A[5][x0][k1c][k2c]: u0, u1, u2, D1 = F0^-1(i k0 u1), D2 = F0^-1(i k0 u2)
+//   P2  omega = i k x u assembled per (k1, k2) (omega1 = i k2 u0 - D2,
+//       omega2 = D1 - i k1 u0), inverse FFT along axis 1
+//       -> B[6][x0][x1][k2c]: u0, u1, u2, w0, w1, w2
+//   P3  per pair of (x0, x1) lines: C2R of the six fields (z = a + i b),
+//       u x omega in registers (optional CFL max), R2C of the three products,
+//       scaled by 1 / (n0 n1 n2) -> nl[3][x0][x1][k2]
+//   P4  forward FFT along axis 1 of nl (generic strided pass)
+//   P5  forward FFT along axis 0 of nl, then the stage update of every mode
+//       of the column (Leray, Nyquist mask, forcing, noise, L, integrator)
+//       writing u_hat: the nonlinear term never returns to HBM.
+#include <cstdlib>
+#include <cstring>
+
+#include "pf_fft.cuh"
 #include "pf_fused.h"
+#include "pf_tma.cuh"
+#include "pf_update.cuh"
 
 namespace pf {
 
-struct FusedPlan {
-  Geo g;
-  int prec;
+template <int N> struct TuneS {  // strided passes P1, P2, P4 (T measured best at 128 / G)
+  static constexpr int E = N <= 16 ? N : (N <= 64 ? 8 : 16);
+  static constexpr int G = N / E;
+  static constexpr int T = (128 / G) < 8 ? 8 : ((128 / G) > 64 ? 64 : 128 / G);
+};
+template <int N> struct TuneU {  // P5 (FFT + update, three fields staged in smem)
+  static constexpr int E = N <= 16 ? N : (N <= 64 ? 8 : 16);
+  static constexpr int G = N / E;
+  static constexpr int T = (256 / G) < 4 ? 4 : ((256 / G) > 64 ? 64 : 256 / G);
+};
+template <int N> struct TuneC {  // contiguous pass P3: 8 values per lane
+  static constexpr int E = 8;
+  static constexpr int G = N / E;   // lanes per line pair, <= 32 for N <= 256
+  static constexpr int PW = 32 / G; // line pairs per warp
+  static constexpr int W = 8;       // warps per CTA
 };
 
-FusedPlan* fused_create(const Geo&, int, int) { return nullptr; }
-void fused_destroy(FusedPlan* p) { delete p; }
-cudaError_t fused_nonlinear(FusedPlan*, const void*, void*, unsigned long long*, cudaStream_t) {
-  return cudaErrorNotSupported;
+struct FGeo {
+  int n0, n1, n2, nh;
+  int c1, c2;
+  int kmax0, kmax1, kmax2;
+  double ks0, ks1, ks2;
+  double cflw0, cflw1, cflw2;  // n_i / L_i
+  long long nspec;
+};
+
+struct FusedPlan {
+  Geo g;
+  FGeo f;
+  int prec;
+  void* A = nullptr;  // 5 * n0 * c1 * c2 complex
+  void* B = nullptr;  // 6 * n0 * n1 * c2 complex
+  int* err = nullptr; // device error word (bounded waits that gave up)
+  int nsm = 148;
+  int var[6] = {0, 0, 0, 0, 0, 0};  // launch variant per pass
+};
+
+// ---------------------------------------------------------------------- P1
+template <typename R, int N, int E, int T>
+__global__ void __launch_bounds__(T * (N / E))
+k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
+     const cx<R>* __restrict__ tw) {
+  constexpr int G = N / E;
+  using C = cx<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
+  const int t = threadIdx.x, j = threadIdx.y;
+  const long long ncols = (long long)f.c1 * f.c2;
+  const long long q = (long long)blockIdx.x * T + t;
+  const bool active = q < ncols;
+  long long in_off = 0;
+  if (active) {
+    const int k1c = (int)(q / f.c2);
+    const int k2c = (int)(q - (long long)k1c * f.c2);
+    const int i1 = k1c <= f.kmax1 ? k1c : k1c + (f.n1 - f.c1);
+    in_off = (long long)i1 * f.nh + k2c;
+  }
+  const long long row_in = (long long)f.n1 * f.nh;
+  const long long fs_out = (long long)N * ncols;
+  auto smf = [&](int pos) -> C& { return sm[pos * T + t]; };
+  auto sync = [] { __syncthreads(); };
+  R k0[E];
+  bool keep[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int kf = kfreq(j + G * e, N);
+    keep[e] = active && abs(kf) <= f.kmax0;
+    k0[e] = (R)(f.ks0 * kf);
+  }
+  C v[E], w[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e)
+    v[e] = keep[e] ? uh[(long long)(j + G * e) * row_in + in_off] : czero<C>();
+  fft<N, E, +1>(v, j, tw, smf, sync);
+  if (active) {
+#pragma unroll
+    for (int e = 0; e < E; ++e) A[(long long)(j + G * e) * ncols + q] = v[e];
+  }
+#pragma unroll
+  for (int c = 1; c <= 2; ++c) {
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      v[e] = keep[e] ? uh[c * f.nspec + (long long)(j + G * e) * row_in + in_off] : czero<C>();
+      w[e] = cmuli(cscale(v[e], k0[e]));
+    }
+    fft<N, E, +1>(v, j, tw, smf, sync);
+    fft<N, E, +1>(w, j, tw, smf, sync);
+    if (active) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        A[c * fs_out + (long long)(j + G * e) * ncols + q] = v[e];
+        A[(2 + c) * fs_out + (long long)(j + G * e) * ncols + q] = w[e];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------- P2
+template <typename R, int N, int E, int T>
+__global__ void __launch_bounds__(T * (N / E))
+k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
+     const cx<R>* __restrict__ tw) {
+  constexpr int G = N / E;
+  using C = cx<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
+  const int t = threadIdx.x, j = threadIdx.y;
+  const long long ncols = (long long)f.n0 * f.c2;
+  const long long q = (long long)blockIdx.x * T + t;
+  const bool active = q < ncols;
+  long long in_base = 0, out_base = 0;
+  R k2 = 0;
+  if (active) {
+    const int x0 = (int)(q / f.c2);
+    const int k2c = (int)(q - (long long)x0 * f.c2);
+    in_base = (long long)x0 * f.c1 * f.c2 + k2c;
+    out_base = (long long)x0 * N * f.c2 + k2c;
+    k2 = (R)(f.ks2 * k2c);
+  }
+  const long long fs_in = (long long)f.n0 * f.c1 * f.c2;
+  const long long fs_out = (long long)f.n0 * N * f.c2;
+  auto smf = [&](int pos) -> C& { return sm[pos * T + t]; };
+  auto sync = [] { __syncthreads(); };
+  R k1[E];
+  long long in_off[E];
+  bool keep[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int i1 = j + G * e;
+    const int kf = kfreq(i1, N);
+    keep[e] = active && abs(kf) <= f.kmax1;
+    k1[e] = (R)(f.ks1 * kf);
+    const int k1c = i1 <= f.kmax1 ? i1 : i1 - (N - f.c1);
+    in_off[e] = in_base + (long long)k1c * f.c2;
+  }
+  auto store = [&](int fld, const C (&v)[E]) {
+    if (active) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) B[fld * fs_out + out_base + (long long)(j + G * e) * f.c2] = v[e];
+    }
+  };
+  C a[E], b[E], w[E];
+  // omega0 = i (k1 u2 - k2 u1); u1; u2
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    a[e] = keep[e] ? A[1 * fs_in + in_off[e]] : czero<C>();
+    b[e] = keep[e] ? A[2 * fs_in + in_off[e]] : czero<C>();
+    w[e] = cmuli(csub(cscale(b[e], k1[e]), cscale(a[e], k2)));
+  }
+  fft<N, E, +1>(w, j, tw, smf, sync);
+  store(3, w);
+  fft<N, E, +1>(a, j, tw, smf, sync);
+  store(1, a);
+  fft<N, E, +1>(b, j, tw, smf, sync);
+  store(2, b);
+  // omega2 = D1 - i k1 u0; omega1 = i k2 u0 - D2; u0
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    a[e] = keep[e] ? A[0 * fs_in + in_off[e]] : czero<C>();
+    b[e] = keep[e] ? A[3 * fs_in + in_off[e]] : czero<C>();
+    w[e] = csub(b[e], cmuli(cscale(a[e], k1[e])));
+  }
+  fft<N, E, +1>(w, j, tw, smf, sync);
+  store(5, w);
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    b[e] = keep[e] ? A[4 * fs_in + in_off[e]] : czero<C>();
+    w[e] = csub(cmuli(cscale(a[e], k2)), b[e]);
+  }
+  fft<N, E, +1>(w, j, tw, smf, sync);
+  store(4, w);
+  fft<N, E, +1>(a, j, tw, smf, sync);
+  store(0, a);
+}
+
+// ---------------------------------------------------------------------- P3
+// Persistent: every warp walks groups of PW = 32 / G line pairs (one pair per
+// G lanes).  A group's six input fields are two adjacent lines each, so one
+// bulk copy per field lands a group in shared memory; the copy of the next
+// group (other stage) is in flight while the current one is transformed.
+template <typename R, int N>
+__global__ void __launch_bounds__(256, 1)
+k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
+     const cx<R>* __restrict__ tw, unsigned long long* __restrict__ maxbits, R scale,
+     int* __restrict__ err, long long ngroups) {
+  constexpr int E = TuneC<N>::E, G = TuneC<N>::G, PW = TuneC<N>::PW, W = TuneC<N>::W;
+  constexpr int H = N / 2;
+  constexpr int SH = sizeof(R) == 4 ? 4 : 3;
+  constexpr int BUF = N + (N >> SH) + 1;
+  static_assert(G <= 32 && 32 % G == 0, "line pairs tile a warp");
+  using C = cx<R>;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int pw = lane / G, j = lane % G;
+  const int fb = 2 * PW * f.c2;        // complex values of one field of a group
+  const int SC = 6 * fb;               // one stage
+  const int WC = ((2 * SC + PW * BUF) + 15) & ~15;
+  const uint32_t fbytes = (uint32_t)(fb * sizeof(C));
+  const long long fs_in = (long long)f.n0 * f.n1 * f.c2;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smraw) + 2 * warp;
+  C* wbase = reinterpret_cast<C*>(smraw + 128) + (long long)warp * WC;
+  C* ex = wbase + 2 * SC + pw * BUF;
+  if (lane == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+  auto issue = [&](long long grp, int s) {
+    if (lane == 0) {
+      mbar_arrive_expect_tx(&bars[s], 6 * fbytes);
+      const C* src = B + grp * fb;
+      C* dst = wbase + s * SC;
+#pragma unroll
+      for (int fld = 0; fld < 6; ++fld) bulk_g2s(dst + fld * fb, src + fld * fs_in, fbytes, &bars[s]);
+    }
+  };
+  auto smf = [&](int pos) -> C& { return ex[pos + (pos >> SH)]; };
+  auto sync = [] { __syncwarp(); };
+  const long long TW = (long long)gridDim.x * W;
+  long long g = (long long)blockIdx.x * W + warp;
+  if (g < ngroups) issue(g, 0);
+  double mx = 0.0;
+  const R h = R(0.5) * scale;
+  for (int it = 0; g < ngroups; g += TW, ++it) {
+    const int s = it & 1;
+    const bool more = g + TW < ngroups;
+    if (more) {
+      __syncwarp();
+      issue(g + TW, s ^ 1);
+    }
+    const bool ok = mbar_wait_bounded(&bars[s], (uint32_t)((it >> 1) & 1));
+    if (!__all_sync(0xffffffffu, ok)) {
+      if (lane == 0) atomicExch(err, kErrWaitP3);
+      if (more) mbar_wait_bounded(&bars[s ^ 1], (uint32_t)(((it + 1) >> 1) & 1));
+      return;
+    }
+    const C* in = wbase + s * SC + 2 * pw * f.c2;
+    C z[6][E];
+#pragma unroll
+    for (int fld = 0; fld < 6; ++fld) {
+      const C* pa = in + fld * fb;
+      const C* pb = pa + f.c2;
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int m = j + G * e;
+        const int k = m <= H ? m : N - m;
+        const bool kin = k < f.c2;
+        C a = kin ? pa[k] : czero<C>();
+        C b = kin ? pb[k] : czero<C>();
+        if (m == 0) { a.y = 0; b.y = 0; }
+        C r;
+        if (m <= H) { r.x = a.x - b.y; r.y = a.y + b.x; }
+        else { r.x = a.x + b.y; r.y = b.x - a.y; }
+        z[fld][e] = r;
+      }
+      fft<N, E, +1>(z[fld], j, tw, smf, sync);
+    }
+    // u x omega for both lines (real parts: line a, imaginary parts: line b)
+    C c[3][E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const C u0 = z[0][e], u1 = z[1][e], u2 = z[2][e];
+      const C w0 = z[3][e], w1 = z[4][e], w2 = z[5][e];
+      c[0][e].x = u1.x * w2.x - u2.x * w1.x;  c[0][e].y = u1.y * w2.y - u2.y * w1.y;
+      c[1][e].x = u2.x * w0.x - u0.x * w2.x;  c[1][e].y = u2.y * w0.y - u0.y * w2.y;
+      c[2][e].x = u0.x * w1.x - u1.x * w0.x;  c[2][e].y = u0.y * w1.y - u1.y * w0.y;
+      if (maxbits) {
+        const double sa = fabs((double)u0.x) * f.cflw0 + fabs((double)u1.x) * f.cflw1 +
+                          fabs((double)u2.x) * f.cflw2;
+        const double sb = fabs((double)u0.y) * f.cflw0 + fabs((double)u1.y) * f.cflw1 +
+                          fabs((double)u2.y) * f.cflw2;
+        mx = fmax(mx, fmax(sa, sb));
+      }
+    }
+    const long long la = 2 * (g * PW + pw);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      fft<N, E, -1>(c[i], j, tw, smf, sync);
+#pragma unroll
+      for (int e = 0; e < E; ++e) smf(j + G * e) = c[i][e];
+      sync();
+      C* oa = nl + i * f.nspec + la * f.nh;
+      C* ob = oa + f.nh;
+#pragma unroll
+      for (int e = 0; e <= E / 2; ++e) {
+        const int k = j + G * e;
+        if (k <= H) {
+          const C zk = smf(k);
+          const C zn = smf((N - k) & (N - 1));
+          C Av, Bv;
+          Av.x = (zk.x + zn.x) * h; Av.y = (zk.y - zn.y) * h;
+          Bv.x = (zk.y + zn.y) * h; Bv.y = -(zk.x - zn.x) * h;
+          oa[k] = Av;
+          ob[k] = Bv;
+        }
+      }
+      sync();
+    }
+  }
+  if (maxbits) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) atomicMax(maxbits, (unsigned long long)__double_as_longlong(mx));
+  }
+}
+
+// ---------------------------------------------------------------------- P4
+// In-place forward FFT along axis 1 of nl[3][x0][x1][k2]: column q = (plane,
+// k2) with plane = comp * n0 + x0.
+template <typename R, int N, int E, int T>
+__global__ void __launch_bounds__(T * (N / E))
+k_p4(cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
+  constexpr int G = N / E;
+  using C = cx<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* sm = reinterpret_cast<C*>(smraw);
+  const int t = threadIdx.x, j = threadIdx.y;
+  const long long ncols = (long long)3 * f.n0 * f.nh;
+  const long long q = (long long)blockIdx.x * T + t;
+  const bool active = q < ncols;
+  long long base = 0;
+  if (active) {
+    const long long pl = q / f.nh;
+    base = pl * N * f.nh + (q - pl * f.nh);
+  }
+  C v[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e)
+    v[e] = active ? nl[base + (long long)(j + G * e) * f.nh] : czero<C>();
+  fft<N, E, -1>(v, j, tw, [&](int pos) -> C& { return sm[pos * T + t]; },
+                [] { __syncthreads(); });
+  if (active) {
+#pragma unroll
+    for (int e = 0; e < E; ++e) nl[base + (long long)(j + G * e) * f.nh] = v[e];
+  }
+}
+
+// ---------------------------------------------------------------------- P5
+// The three FFT outputs of a column tile are parked in shared memory (one
+// N x T buffer per component, also the FFT's exchange buffer) so the update
+// phase holds only a chunk of modes in registers; u_hat / u0 of a chunk are
+// loaded before any of its stores.
+template <typename R, int N, int NC, bool NOISE>
+__global__ void __launch_bounds__(TuneU<N>::T * TuneU<N>::G)
+k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
+  constexpr int E = TuneU<N>::E, G = TuneU<N>::G, T = TuneU<N>::T;
+  constexpr int CH = E < 4 ? E : 4;
+  using C = cx<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C* S = reinterpret_cast<C*>(smraw);
+  const int t = threadIdx.x, j = threadIdx.y;
+  const int ncols = f.n1 * f.nh;
+  const int q = blockIdx.x * T + t;
+  const bool active = q < ncols;
+  auto sync = [] { __syncthreads(); };
+#pragma unroll 1
+  for (int c = 0; c < 3; ++c) {
+    C* Sc = S + c * N * T;
+    auto smf = [&](int pos) -> C& { return Sc[pos * T + t]; };
+    C v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+      v[e] = active ? nl[c * f.nspec + (long long)(j + G * e) * ncols + q] : czero<C>();
+    fft<N, E, -1>(v, j, tw, smf, sync);
+#pragma unroll
+    for (int e = 0; e < E; ++e) Sc[(j + G * e) * T + t] = v[e];
+  }
+  const StageScalars<R> sc = stage_scalars<R>(U);
+  double accE = 0.0, accZ = 0.0;
+  if (active) {
+    const int i1 = q / f.nh, i2 = q - i1 * f.nh;
+    const R k1 = (R)(f.ks1 * kfreq(i1, f.n1)), k2 = (R)(f.ks2 * i2);
+    cx<R>* __restrict__ uh = U.uhat;
+    const cx<R>* __restrict__ u0p = U.u0;
+    const long long ns = f.nspec;
+#pragma unroll
+    for (int e0 = 0; e0 < E; e0 += CH) {
+      C un[CH][3], u0v[CH][3];
+#pragma unroll
+      for (int cc = 0; cc < CH; ++cc) {
+        const long long m = (long long)(j + G * (e0 + cc)) * ncols + q;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          un[cc][a] = uh[a * ns + m];
+          u0v[cc][a] = U.save_u0 ? un[cc][a] : u0p[a * ns + m];
+        }
+      }
+#pragma unroll
+      for (int cc = 0; cc < CH; ++cc) {
+        const int i0 = j + G * (e0 + cc);
+        const long long m = (long long)i0 * ncols + q;
+        ModeK<R, 3> mk_;
+        mk_.ix.i0 = i0; mk_.ix.i1 = i1; mk_.ix.i2 = i2;
+        const R k0 = (R)(f.ks0 * kfreq(i0, N));
+        mk_.k[0] = k0; mk_.k[1] = k1; mk_.k[2] = k2;
+        mk_.k2 = k0 * k0 + k1 * k1 + k2 * k2;
+        C nv[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) nv[a] = S[a * N * T + i0 * T + t];
+        update_core<R, 3, NC, NOISE>(U, m, mk_, nv, true, un[cc], u0v[cc], sc, accE, accZ);
+      }
+    }
+  }
+  if (U.diag) block_add2(accE, accZ, U.diag);
+}
+
+// ------------------------------------------------------------------ plan / launch
+// Raise the dynamic shared-memory limit when dynamic plus the kernel's static
+// shared memory (up to 1 KB here) could pass the 48 KB default.
+template <typename K> static cudaError_t set_smem(K kern, size_t bytes) {
+  if (bytes + 1024 > 48 * 1024)
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  return cudaSuccess;
+}
+
+static bool pow2(int n) { return n >= 16 && (n & (n - 1)) == 0; }
+
+FusedPlan* fused_create(const Geo& g, int precision, int dealias) {
+  if (g.dim != 3 || precision != 0 || dealias != 0) return nullptr;
+  for (int a = 0; a < 3; ++a)
+    if (!pow2(g.n[a]) || g.n[a] > 512) return nullptr;
+  if (g.n[2] > 256) return nullptr;
+  FusedPlan* p = new FusedPlan();
+  p->g = g;
+  p->prec = precision;
+  FGeo& f = p->f;
+  f.n0 = g.n[0]; f.n1 = g.n[1]; f.n2 = g.n[2]; f.nh = g.nh;
+  f.kmax0 = g.kmax[0]; f.kmax1 = g.kmax[1]; f.kmax2 = g.kmax[2];
+  f.c1 = 2 * f.kmax1 + 1;
+  f.c2 = f.kmax2 + 1;
+  f.ks0 = g.kscale[0]; f.ks1 = g.kscale[1]; f.ks2 = g.kscale[2];
+  f.cflw0 = g.n[0] * g.kscale[0] / (2.0 * M_PI);
+  f.cflw1 = g.n[1] * g.kscale[1] / (2.0 * M_PI);
+  f.cflw2 = g.n[2] * g.kscale[2] / (2.0 * M_PI);
+  f.nspec = g.nspec;
+  if (const char* v = getenv("PF_FUSED_VARIANT")) {
+    // "p1:1,p2:2,p4:1"
+    for (const char* c = v; *c; ++c)
+      if (c[0] == 'p' && c[1] >= '1' && c[1] <= '5' && c[2] == ':') p->var[c[1] - '0'] = atoi(c + 3);
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, dev);
+  const size_t cb = precision == 0 ? 8 : 16;
+  const size_t a_el = 5ull * f.n0 * f.c1 * f.c2, b_el = 6ull * f.n0 * f.n1 * f.c2;
+  if (cudaMalloc(&p->A, cb * a_el) != cudaSuccess || cudaMalloc(&p->B, cb * b_el) != cudaSuccess ||
+      cudaMalloc(&p->err, sizeof(int)) != cudaSuccess ||
+      cudaMemset(p->err, 0, sizeof(int)) != cudaSuccess) {
+    fused_destroy(p);
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+
+void fused_destroy(FusedPlan* p) {
+  if (!p) return;
+  if (p->A) cudaFree(p->A);
+  if (p->B) cudaFree(p->B);
+  if (p->err) cudaFree(p->err);
+  delete p;
+}
+
+#define PF_SWITCH_S(n, CALL)      \
+  switch (n) {                    \
+    case 16: return CALL(16);     \
+    case 32: return CALL(32);     \
+    case 64: return CALL(64);     \
+    case 128: return CALL(128);   \
+    case 256: return CALL(256);   \
+    case 512: return CALL(512);   \
+    default: return cudaErrorInvalidValue; \
+  }
+
+// Launch variants (radix width E, columns per CTA T) of the strided passes;
+// variant 0 is the default of TuneS, 1..3 exist for n = 256 (tuning knob
+// PF_FUSED_VARIANT="p1:v,p2:v,p4:v").
+template <int N, int E, int T> static cudaError_t p1_run(FusedPlan* p, const float2* uh,
+                                                        cudaStream_t st) {
+  constexpr int G = N / E;
+  const float2* tw = tw_base<float>() + (N - 2);
+  const long long ncols = (long long)p->f.c1 * p->f.c2;
+  const size_t sm = G > 1 ? sizeof(float2) * N * T : 0;
+  cudaError_t e = set_smem(k_p1<float, N, E, T>, sm);
+  if (e != cudaSuccess) return e;
+  k_p1<float, N, E, T><<<(unsigned)((ncols + T - 1) / T), dim3(T, G), sm, st>>>(
+      uh, (float2*)p->A, p->f, tw);
+  return launched();
+}
+
+template <int N, int E, int T> static cudaError_t p2_run(FusedPlan* p, cudaStream_t st) {
+  constexpr int G = N / E;
+  const float2* tw = tw_base<float>() + (N - 2);
+  const long long ncols = (long long)p->f.n0 * p->f.c2;
+  const size_t sm = G > 1 ? sizeof(float2) * N * T : 0;
+  cudaError_t e = set_smem(k_p2<float, N, E, T>, sm);
+  if (e != cudaSuccess) return e;
+  k_p2<float, N, E, T><<<(unsigned)((ncols + T - 1) / T), dim3(T, G), sm, st>>>(
+      (const float2*)p->A, (float2*)p->B, p->f, tw);
+  return launched();
+}
+
+template <int N, int E, int T> static cudaError_t p4_run(FusedPlan* p, float2* nl,
+                                                        cudaStream_t st) {
+  constexpr int G = N / E;
+  const float2* tw = tw_base<float>() + (N - 2);
+  const long long ncols = (long long)3 * p->f.n0 * p->f.nh;
+  const size_t sm = G > 1 ? sizeof(float2) * N * T : 0;
+  cudaError_t e = set_smem(k_p4<float, N, E, T>, sm);
+  if (e != cudaSuccess) return e;
+  k_p4<float, N, E, T><<<(unsigned)((ncols + T - 1) / T), dim3(T, G), sm, st>>>(nl, p->f, tw);
+  return launched();
+}
+
+#define PF_VARIANTS(RUN, N, ...)                                        \
+  if constexpr (N == 256) {                                             \
+    switch (var) {                                                      \
+      case 1: return RUN<256, 8, 16>(__VA_ARGS__);                      \
+      case 2: return RUN<256, 8, 32>(__VA_ARGS__);                      \
+      case 3: return RUN<256, 16, 8>(__VA_ARGS__);                      \
+      default: break;                                                   \
+    }                                                                   \
+  }                                                                     \
+  return RUN<N, TuneS<N>::E, TuneS<N>::T>(__VA_ARGS__);
+
+template <int N> static cudaError_t p1_n(FusedPlan* p, const float2* uh, cudaStream_t st) {
+  const int var = p->var[1];
+  PF_VARIANTS(p1_run, N, p, uh, st)
+}
+template <int N> static cudaError_t p2_n(FusedPlan* p, cudaStream_t st) {
+  const int var = p->var[2];
+  PF_VARIANTS(p2_run, N, p, st)
+}
+template <int N> static cudaError_t p4_n(FusedPlan* p, float2* nl, cudaStream_t st) {
+  const int var = p->var[4];
+  PF_VARIANTS(p4_run, N, p, nl, st)
+}
+
+template <int N>
+static cudaError_t p3_n(FusedPlan* p, float2* nl, unsigned long long* maxbits, cudaStream_t st) {
+  if constexpr (N > 256) {
+    return cudaErrorInvalidValue;
+  } else {
+    using TN = TuneC<N>;
+    const float2* tw = tw_base<float>() + (N - 2);
+    const long long ngroups = (long long)p->f.n0 * p->f.n1 / (2 * TN::PW);
+    const int fb = 2 * TN::PW * p->f.c2;
+    const int WC = ((2 * 6 * fb + TN::PW * (N + (N >> 4) + 1)) + 15) & ~15;
+    const size_t sm = 128 + sizeof(float2) * (size_t)TN::W * WC;
+    cudaError_t e = set_smem(k_p3<float, N>, sm);
+    if (e != cudaSuccess) return e;
+    const float scale = (float)(1.0 / ((double)p->f.n0 * p->f.n1 * p->f.n2));
+    long long blocks = (ngroups + TN::W - 1) / TN::W;
+    if (blocks > p->nsm) blocks = p->nsm;
+    k_p3<float, N><<<(unsigned)blocks, 32 * TN::W, sm, st>>>(
+        (const float2*)p->B, nl, p->f, tw, maxbits, scale, p->err, ngroups);
+    return launched();
+  }
+}
+
+template <int N>
+static cudaError_t p5_n(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, const float2* nl,
+                        cudaStream_t st) {
+  using TN = TuneU<N>;
+  const float2* tw = tw_base<float>() + (N - 2);
+  const long long ncols = (long long)p->f.n1 * p->f.nh;
+  const size_t sm = sizeof(float2) * 3 * N * TN::T;
+  const dim3 grid((unsigned)((ncols + TN::T - 1) / TN::T)), block(TN::T, TN::G);
+  cudaError_t e;
+  if (U.noise_src == kNoiseNone) {
+    e = set_smem(k_p5<float, N, 3, false>, sm);
+    if (e != cudaSuccess) return e;
+    k_p5<float, N, 3, false><<<grid, block, sm, st>>>(U, nl, p->f, tw);
+  } else if (ncomp == 9) {
+    e = set_smem(k_p5<float, N, 9, true>, sm);
+    if (e != cudaSuccess) return e;
+    k_p5<float, N, 9, true><<<grid, block, sm, st>>>(U, nl, p->f, tw);
+  } else {
+    e = set_smem(k_p5<float, N, 3, true>, sm);
+    if (e != cudaSuccess) return e;
+    k_p5<float, N, 3, true><<<grid, block, sm, st>>>(U, nl, p->f, tw);
+  }
+  return launched();
+}
+
+cudaError_t fused_pass(FusedPlan* p, int pass, const void* uhat, void* nl,
+                       unsigned long long* maxbits, cudaStream_t st) {
+  if (!p || !tw_base<float>()) return cudaErrorNotReady;
+  switch (pass) {
+    case 1: {
+#define PF_CALL(NN) p1_n<NN>(p, (const float2*)uhat, st)
+      PF_SWITCH_S(p->f.n0, PF_CALL)
+#undef PF_CALL
+    }
+    case 2: {
+#define PF_CALL(NN) p2_n<NN>(p, st)
+      PF_SWITCH_S(p->f.n1, PF_CALL)
+#undef PF_CALL
+    }
+    case 3: {
+#define PF_CALL(NN) p3_n<NN>(p, (float2*)nl, maxbits, st)
+      PF_SWITCH_S(p->f.n2, PF_CALL)
+#undef PF_CALL
+    }
+    case 4: {
+#define PF_CALL(NN) p4_n<NN>(p, (float2*)nl, st)
+      PF_SWITCH_S(p->f.n1, PF_CALL)
+#undef PF_CALL
+    }
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t fused_update(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, const void* nl,
+                         cudaStream_t st) {
+  if (!p || !tw_base<float>()) return cudaErrorNotReady;
+#define PF_CALL(NN) p5_n<NN>(p, U, ncomp, (const float2*)nl, st)
+  PF_SWITCH_S(p->f.n0, PF_CALL)
+#undef PF_CALL
+}
+
+int fused_device_error(FusedPlan* p) {
+  if (!p || !p->err) return 0;
+  int v = 0;
+  if (cudaMemcpy(&v, p->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  return v;
 }
 
 }  // namespace pf

@@ -1,17 +1,24 @@
-// Fused pencil passes of the nonlinear term (u x omega with 2/3 truncation).
+// Fused pencil passes of the 3D nonlinear term (u x omega with the 2/3 rule).
 #pragma once
-#include "pf_internal.h"
+#include "pf_kernels.h"
 
 namespace pf {
 
 struct FusedPlan;
 
-// Returns nullptr when no fused schedule is built for this geometry.
+// Returns nullptr when no fused schedule is built for this geometry
+// (3D, FP32, 2/3 rule, power-of-two sides 16..512 with n2 <= 256).
 FusedPlan* fused_create(const Geo& g, int precision, int dealias);
 void fused_destroy(FusedPlan* p);
-// Unprojected nonlinear term of uhat into nl; optional max(sum |u_i|/dx_i)
-// as float bits into maxbits.
-cudaError_t fused_nonlinear(FusedPlan* p, const void* uhat, void* nl, unsigned long long* maxbits,
-                            cudaStream_t st);
+// Pass 1..4 of the nonlinear term of uhat (unprojected) into nl; pass 3
+// writes max(sum_i |u_i| / dx_i) as double bits into maxbits when non-null.
+cudaError_t fused_pass(FusedPlan* p, int pass, const void* uhat, void* nl,
+                       unsigned long long* maxbits, cudaStream_t st);
+// Pass 5: forward FFT along axis 0 of nl fused with the stage update.
+cudaError_t fused_update(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, const void* nl,
+                         cudaStream_t st);
+
+// Error word of bounded device waits (0: none; synchronous read).
+int fused_device_error(FusedPlan* p);
 
 }  // namespace pf

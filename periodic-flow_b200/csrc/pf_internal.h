@@ -8,6 +8,14 @@
 
 namespace pf {
 
+// kernel launch accounting: every launcher of this library reports here
+void count_launch();
+long long launch_total();
+inline cudaError_t launched() {
+  count_launch();
+  return cudaGetLastError();
+}
+
 // twiddle tables: filled once per device before any FFT launch
 cudaError_t ensure_tables();
 // device address of the concatenated tables of the current device; the table

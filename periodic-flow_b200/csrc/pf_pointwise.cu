@@ -11,7 +11,7 @@
 #include <cstdio>
 
 #include "pf_kernels.h"
-#include "pf_mode.cuh"
+#include "pf_update.cuh"
 
 namespace pf {
 
@@ -24,149 +24,19 @@ static unsigned grid_for(long long n, int per_block = kBlock, long long cap = 14
   return (unsigned)b;
 }
 
-// FP64 block reduction of two partial sums into gl[0], gl[1].
-PF_D void block_add2(double a, double b, double* gl) {
-  __shared__ double sa[32], sb[32];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    a += __shfl_xor_sync(0xffffffffu, a, o);
-    b += __shfl_xor_sync(0xffffffffu, b, o);
-  }
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) { sa[w] = a; sb[w] = b; }
-  __syncthreads();
-  if (w == 0) {
-    const int nw = (blockDim.x + 31) >> 5;
-    a = l < nw ? sa[l] : 0.0;
-    b = l < nw ? sb[l] : 0.0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      a += __shfl_xor_sync(0xffffffffu, a, o);
-      b += __shfl_xor_sync(0xffffffffu, b, o);
-    }
-    if (l == 0) { atomicAdd(gl, a); atomicAdd(gl + 1, b); }
-  }
-}
-
-template <typename R, int D> struct ModeK {
-  R k[D];
-  R k2;
-  KInt<D> ki;
-  ModeIdx ix;
-};
-
-template <typename R, int D> PF_D ModeK<R, D> mode_k(const Geo& g, long long m) {
-  ModeK<R, D> r;
-  r.ix = mode_index(g, m);
-  r.ki = kint_of<D>(g, r.ix);
-  double k2 = 0.0;
-#pragma unroll
-  for (int a = 0; a < D; ++a) {
-    const double ka = g.kscale[a] * (double)r.ki.k[a];
-    r.k[a] = (R)ka;
-    k2 += ka * ka;
-  }
-  r.k2 = (R)k2;
-  return r;
-}
-
-PF_D double half_weight(const Geo& g, const ModeIdx& ix) {
-  const int il = g.dim == 3 ? ix.i2 : ix.i1;
-  const int nl = g.n[g.dim - 1];
-  return (il == 0 || ((nl % 2 == 0) && il == nl / 2)) ? 1.0 : 2.0;
-}
-
-// Normal factor of the noise draws: mask(k != 0) / sqrt(prod N) / sqrt(2 - 2/d)
-// (space_solver.py:143-145), passed in as nf.
-template <typename R, int D, int NC>
-PF_D void load_noise(const UpdateArgs<R>& A, long long m, const ModeK<R, D>& mk_,
-                     cx<R> (&w1)[NC], cx<R> (&w2)[NC]) {
-  if (A.noise_src == kNoiseInjected) {
-#pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      w1[c] = A.winj[(long long)c * A.g.nspec + m];
-      w2[c] = A.winj[(long long)(NC + c) * A.g.nspec + m];
-    }
-  } else {
-    const DrawSite s = draw_site(A.g, mk_.ix.i0, mk_.ix.i1, mk_.ix.i2);
-    const R nf = mk_.k2 == R(0) ? R(0) : (R)A.noise_norm;
-#pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      w1[c] = cscale(draw_value<R>(s, c, A.seed, A.step), nf);
-      w2[c] = cscale(draw_value<R>(s, NC + c, A.seed, A.step), nf);
-    }
-  }
-}
-
 template <typename R, int D, int NC>
 __global__ void __launch_bounds__(kBlock) k_update(UpdateArgs<R> A) {
   using C = cx<R>;
   const Geo& g = A.g;
-  const R dt = (R)A.dscal[kScalDt];
-  const R sqdt = (R)sqrt(A.dscal[kScalDt]);
-  R fcoef = R(0);
-  if (A.forcing) {
-    const double ef = A.dscal[kScalBandE];
-    fcoef = ef > 0.0 ? (R)(A.f_eps / (2.0 * ef)) : R(0);
-  }
+  const StageScalars<R> sc = stage_scalars<R>(A);
   double accE = 0.0, accZ = 0.0;
   for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < g.nspec;
        m += (long long)gridDim.x * blockDim.x) {
     const ModeK<R, D> mk_ = mode_k<R, D>(g, m);
-    C un[D], u0v[D], nv[D], xi[D];
+    C nv[D];
 #pragma unroll
-    for (int a = 0; a < D; ++a) {
-      un[a] = A.uhat[a * g.nspec + m];
-      u0v[a] = A.save_u0 ? un[a] : A.u0[a * g.nspec + m];
-    }
-    if (A.save_u0) {
-#pragma unroll
-      for (int a = 0; a < D; ++a) A.u0[a * g.nspec + m] = un[a];
-    }
-    // nonlinear term: Leray projection and optional Nyquist mask
-    // (space_solver.py:297-300)
-    if (A.nl) {
-#pragma unroll
-      for (int a = 0; a < D; ++a) nv[a] = A.nl[a * g.nspec + m];
-      leray<R, D>(nv, mk_.k, mk_.k2);
-      if (A.nyq_mask && is_nyquist<D>(g, mk_.ix)) {
-#pragma unroll
-        for (int a = 0; a < D; ++a) nv[a] = czero<C>();
-      }
-    } else {
-#pragma unroll
-      for (int a = 0; a < D; ++a) nv[a] = czero<C>();
-    }
-    // forcing: eps / (2 E_band) u on 0 < |k|^2 <= kf^2
-    if (A.forcing && mk_.k2 > R(0) && (double)mk_.k2 <= A.f_kf2) {
-#pragma unroll
-      for (int a = 0; a < D; ++a) nv[a] = cadd(nv[a], cscale(un[a], fcoef));
-    }
-    // noise
-    if (A.noise_src != kNoiseNone) {
-      C w1[NC], w2[NC];
-      load_noise<R, D, NC>(A, m, mk_, w1, w2);
-      const R corr = A.corr ? A.corr[m] : R(0);
-      noise_term<R, D, NC>(xi, w1, w2, (R)A.coef.a, A.noise_type, mk_.k, mk_.k2, corr, (R)A.noise_mag);
-    } else {
-#pragma unroll
-      for (int a = 0; a < D; ++a) xi[a] = czero<C>();
-    }
-    const R L = A.lop ? A.lop[m] : (R)(-A.nu) * mk_.k2;
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      const C r = stage_update<R>(A.coef, dt, sqdt, L, u0v[a], un[a], nv[a], xi[a]);
-      A.uhat[a * g.nspec + m] = r;
-      un[a] = r;
-    }
-    if (A.diag) {
-      double e = 0.0;
-#pragma unroll
-      for (int a = 0; a < D; ++a) e += (double)un[a].x * un[a].x + (double)un[a].y * un[a].y;
-      const double w = half_weight(g, mk_.ix);
-      accE += 0.5 * w * e;
-      accZ += 0.5 * w * e * (double)mk_.k2;
-    }
+    for (int a = 0; a < D; ++a) nv[a] = A.nl ? A.nl[a * g.nspec + m] : czero<C>();
+    update_mode<R, D, NC>(A, m, mk_, nv, A.nl != nullptr, sc, accE, accZ);
   }
   if (A.diag) block_add2(accE, accZ, A.diag);
 }
@@ -315,12 +185,27 @@ __global__ void k_advance_time(double* dscal, int n) {
   for (int i = 0; i < n; ++i) dscal[kScalTime] += dscal[kScalDt];
 }
 
-// E_band = 1/2 sum_{0<|k|^2<=kf^2} w |u|^2  -> dscal[kScalBandE]
+// E_band = 1/2 sum_{0<|k|^2<=kf^2} w |u|^2  -> dscal[kScalBandE].  Visits only
+// the index box that can hold the band: per axis cnt[a] slots, slot s maps to
+// index s when the whole axis is needed, else to wavenumber s - K (mod n).
+struct BandBox { int cnt[3], K[3], full[3]; long long total; };
+
 template <typename R, int D>
-__global__ void k_band_energy(const cx<R>* __restrict__ u, Geo g, double kf2, double* dscal) {
+__global__ void k_band_energy(const cx<R>* __restrict__ u, Geo g, double kf2, BandBox bx,
+                              double* dscal) {
   double acc = 0.0;
-  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < g.nspec;
-       m += (long long)gridDim.x * blockDim.x) {
+  for (long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x; b < bx.total;
+       b += (long long)gridDim.x * blockDim.x) {
+    int idx[3] = {0, 0, 0};
+    long long r = b;
+    for (int a = D - 1; a >= 0; --a) {
+      const int s = (int)(r % bx.cnt[a]);
+      r /= bx.cnt[a];
+      if (a == D - 1 || bx.full[a]) idx[a] = s;
+      else idx[a] = ((s - bx.K[a]) % g.n[a] + g.n[a]) % g.n[a];
+    }
+    long long m = idx[0];
+    for (int a = 1; a < D; ++a) m = m * g.s[a] + idx[a];
     const ModeK<double, D> q = mode_k<double, D>(g, m);
     if (q.k2 > 0.0 && q.k2 <= kf2) {
       double e = 0.0;
@@ -379,7 +264,7 @@ cudaError_t launch_update(const UpdateArgs<R>& A, int ncomp, cudaStream_t st) {
     if (ncomp == 4) k_update<R, 2, 4><<<grid, kBlock, 0, st>>>(A);
     else k_update<R, 2, 2><<<grid, kBlock, 0, st>>>(A);
   }
-  return cudaGetLastError();
+  return launched();
 }
 
 template <typename R>
@@ -392,7 +277,7 @@ cudaError_t launch_stokes(const StokesArgs<R>& A, int ncomp, cudaStream_t st) {
     if (ncomp == 4) k_stokes<R, 2, 4><<<grid, kBlock, 0, st>>>(A);
     else k_stokes<R, 2, 2><<<grid, kBlock, 0, st>>>(A);
   }
-  return cudaGetLastError();
+  return launched();
 }
 
 template <typename R>
@@ -400,14 +285,14 @@ cudaError_t launch_mask_copy(cx<R>* dst, const cx<R>* src, const Geo& g, int nco
                              cudaStream_t st) {
   if (g.dim == 3) k_mask_copy<R, 3><<<grid_for(g.nspec), kBlock, 0, st>>>(dst, src, g, ncomp);
   else k_mask_copy<R, 2><<<grid_for(g.nspec), kBlock, 0, st>>>(dst, src, g, ncomp);
-  return cudaGetLastError();
+  return launched();
 }
 
 template <typename R>
 cudaError_t launch_curl_masked(cx<R>* dst, const cx<R>* u, const Geo& g, cudaStream_t st) {
   if (g.dim == 3) k_curl_masked<R, 3><<<grid_for(g.nspec), kBlock, 0, st>>>(dst, u, g);
   else k_curl_masked<R, 2><<<grid_for(g.nspec), kBlock, 0, st>>>(dst, u, g);
-  return cudaGetLastError();
+  return launched();
 }
 
 template <typename R>
@@ -415,18 +300,18 @@ cudaError_t launch_cross(R* u, const R* w, const Geo& g, unsigned long long* max
                          cudaStream_t st) {
   if (g.dim == 3) k_cross<R, 3><<<grid_for(g.nphys), kBlock, 0, st>>>(u, w, g, maxbits);
   else k_cross<R, 2><<<grid_for(g.nphys), kBlock, 0, st>>>(u, w, g, maxbits);
-  return cudaGetLastError();
+  return launched();
 }
 
 cudaError_t launch_set_dt(double* dscal, const unsigned long long* maxbits, double cfl,
                           cudaStream_t st) {
   k_set_dt<<<1, 1, 0, st>>>(dscal, maxbits, cfl);
-  return cudaGetLastError();
+  return launched();
 }
 
 cudaError_t launch_advance_time(double* dscal, int n, cudaStream_t st) {
   k_advance_time<<<1, 1, 0, st>>>(dscal, n);
-  return cudaGetLastError();
+  return launched();
 }
 
 template <typename R>
@@ -434,16 +319,34 @@ cudaError_t launch_band_energy(const cx<R>* u, const Geo& g, double kf2, double*
                                cudaStream_t st) {
   cudaError_t e = cudaMemsetAsync(dscal + kScalBandE, 0, sizeof(double), st);
   if (e != cudaSuccess) return e;
-  if (g.dim == 3) k_band_energy<R, 3><<<grid_for(g.nspec), kBlock, 0, st>>>(u, g, kf2, dscal);
-  else k_band_energy<R, 2><<<grid_for(g.nspec), kBlock, 0, st>>>(u, g, kf2, dscal);
-  return cudaGetLastError();
+  BandBox bx;
+  bx.total = 1;
+  const double kf = sqrt(kf2);
+  for (int a = 0; a < 3; ++a) { bx.cnt[a] = 1; bx.K[a] = 0; bx.full[a] = 0; }
+  for (int a = 0; a < g.dim; ++a) {
+    const int K = (int)floor(kf / g.kscale[a] + 1e-9);
+    if (a == g.dim - 1) {
+      bx.cnt[a] = (K < g.nh - 1 ? K : g.nh - 1) + 1;
+    } else if (2 * K + 1 >= g.n[a]) {
+      bx.full[a] = 1;
+      bx.cnt[a] = g.n[a];
+    } else {
+      bx.K[a] = K;
+      bx.cnt[a] = 2 * K + 1;
+    }
+    bx.total *= bx.cnt[a];
+  }
+  const unsigned grid = grid_for(bx.total);
+  if (g.dim == 3) k_band_energy<R, 3><<<grid, kBlock, 0, st>>>(u, g, kf2, bx, dscal);
+  else k_band_energy<R, 2><<<grid, kBlock, 0, st>>>(u, g, kf2, bx, dscal);
+  return launched();
 }
 
 template <typename R>
 cudaError_t launch_energy(const cx<R>* u, const Geo& g, double* out2, cudaStream_t st) {
   if (g.dim == 3) k_energy<R, 3><<<grid_for(g.nspec), kBlock, 0, st>>>(u, g, out2);
   else k_energy<R, 2><<<grid_for(g.nspec), kBlock, 0, st>>>(u, g, out2);
-  return cudaGetLastError();
+  return launched();
 }
 
 template <typename R>
@@ -451,7 +354,7 @@ cudaError_t launch_spectrum(const cx<R>* u, const Geo& g, double* out, int nbins
                             double kunit, cudaStream_t st) {
   if (g.dim == 3) k_spectrum<R, 3><<<grid_for(g.nspec), kBlock, 0, st>>>(u, g, out, nbins, kunit);
   else k_spectrum<R, 2><<<grid_for(g.nspec), kBlock, 0, st>>>(u, g, out, nbins, kunit);
-  return cudaGetLastError();
+  return launched();
 }
 
 #define PF_INST(R)                                                                          \

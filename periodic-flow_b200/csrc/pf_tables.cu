@@ -1,4 +1,5 @@
 // Twiddle tables of the FFT engine, one static copy per device.
+#include <atomic>
 #include <cmath>
 #include <mutex>
 #include <vector>
@@ -7,6 +8,10 @@
 #include "pf_internal.h"
 
 namespace pf {
+
+static std::atomic<long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long long launch_total() { return g_launches.load(std::memory_order_relaxed); }
 
 static __device__ float2 g_tw_f32[kTwSize];
 static __device__ double2 g_tw_f64[kTwSize];

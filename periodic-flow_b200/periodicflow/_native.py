@@ -16,6 +16,8 @@ PF_NOISE_THERMAL, PF_NOISE_CORRELATED = 0, 1
 PF_NOISE_SRC_PHILOX, PF_NOISE_SRC_INJECTED = 1, 2
 PF_DEALIAS_TRUNCATE, PF_DEALIAS_PAD = 0, 1
 PF_FP32, PF_FP64 = 0, 1
+PF_PASS_UPDATE, PF_PASS_FFT_STRIDED, PF_PASS_FFT_LAST, PF_PASS_STOKES = 0, 1, 2, 4
+PF_PASS_FUSED = {1: 11, 2: 12, 3: 13, 4: 14, 5: 15}
 
 
 class PfConfig(C.Structure):
@@ -73,6 +75,10 @@ _SIGS = [
     ("pf_history", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     ("pf_record_history", C.c_int, [C.c_void_p, C.c_int]),
     ("pf_spectrum", C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    ("pf_kernel_timer", C.c_int, [C.c_void_p, C.c_int]),
+    ("pf_kernel_timer_read", C.c_int, [C.c_void_p, C.POINTER(C.c_double),
+                                       C.POINTER(C.c_longlong)]),
+    ("pf_launch_count", C.c_int, [C.POINTER(C.c_longlong)]),
     ("pf_op_cross", C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_longlong)] + [C.c_void_p] * 4),
     ("pf_op_curl", C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_longlong)] + [C.c_void_p] * 4),
     ("pf_op_apply_linear_operator", C.c_int,

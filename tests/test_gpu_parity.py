@@ -214,3 +214,49 @@ def test_forcing_and_cfl_rk3_vs_oracle():
     t, step, dt = s.space_solver.time()
     assert step == 4 and abs(t - o.t) < 1e-12 * o.t and abs(dt - o.dt) < 1e-12 * o.dt
     assert rel_l2(s.space_solver.u_hat, o.u_hat) < 1e-11
+
+
+# ------------------------------------------------------------- fused passes
+@pytest.mark.parametrize("N", [(16, 16, 16), (32, 32, 32), (64, 32, 128), (32, 128, 64),
+                               (128, 128, 128)])
+@pytest.mark.parametrize("integ", ["rk3", "rk4", "implicit_pc"])
+def test_fused_passes_match_oracle(N, integ):
+    """FP32 fused pencil path vs the FP64 oracle after 2 steps (1e-5 target)."""
+    o = O.OracleSolver(N, 2e-3, time_integrator=integ, viscosity=2e-3)
+    uh0 = O.spectral_random_field(o.grid, 7)
+    o.initialize(uh0, "fourier")
+    s = solver(N, dt=2e-3, time_integrator=integ, viscosity=2e-3, precision="fp32", fused=True)
+    s.initialize(uh0, "fourier")
+    o.advance(2)
+    s.space_solver.step(2)
+    assert rel_l2(s.space_solver.u_hat, o.u_hat) < 1e-5
+
+
+def test_fused_forcing_cfl_noise_matches_generic():
+    N = (64, 64, 64)
+    kw = dict(dt=1e-3, time_integrator="rk3", viscosity=2e-3, precision="fp32",
+              forcing=(0.1, 2.5), cfl=0.5, noise_mag=1e-3, seed=3)
+    a = solver(N, fused=True, **kw)
+    b = solver(N, fused=False, **kw)
+    uh0 = O.spectral_random_field(O.Grid(N), 1)
+    a.initialize(uh0, "fourier")
+    b.initialize(uh0, "fourier")
+    a.space_solver.step(3)
+    b.space_solver.step(3)
+    ta, sa, da = a.space_solver.time()
+    tb, sb, db = b.space_solver.time()
+    assert sa == sb == 3 and abs(da - db) < 1e-5 * db
+    assert rel_l2(a.space_solver.u_hat, b.space_solver.u_hat) < 2e-6
+
+
+def test_fused_energy_history_matches_oracle():
+    N = (64, 64, 64)
+    o = O.OracleSolver(N, 5e-3, time_integrator="rk4", viscosity=1 / 1600)
+    o.initialize(O.taylor_green(o.grid))
+    s = solver(N, dt=5e-3, time_integrator="rk4", viscosity=1 / 1600, precision="fp32",
+               diagnostics=True, fused=True)
+    s.initialize(O.taylor_green(o.grid))
+    ho = np.array(o.advance(5, diagnostics=True))
+    s.space_solver.step(5)
+    hs = s.space_solver.history()
+    assert np.max(np.abs(hs - ho) / np.abs(ho)) < 1e-5
