@@ -157,6 +157,23 @@ int pf_kernel_timer_read(pf_solver* h, double* total_ms, long long* launches);
 /* Total kernels launched by this library in this process. */
 int pf_launch_count(long long* count);
 
+/* ---- backward transform without device allocation ----------------------
+ * No counterpart in the reference: an addition for callers that cannot call
+ * cudaMalloc (a fixed memory budget handed over by an embedding application,
+ * a context where the allocator must not be entered, up-front accounting of
+ * every allocation).  Same result as pf_get_physical (the reference's
+ * V.backward, space_solver.py:221-225) for a spectral field the caller already
+ * holds on the device: u_hat (dim, spectral) complex and u (dim, n...) real,
+ * both device arrays of the given precision.  The transform's work copy lives
+ * in one fixed 32 MiB device array of the library (held by every GPU that
+ * loads it until exit): requests needing more than dim * nspec complex values
+ * of 32 MiB are rejected with PF_ERR_INVALID.  The first call on a device sets
+ * up that array's address and the FFT tables -- make it before any stream
+ * capture.  Calls share the array, so calls that overlap on the GPU race;
+ * serialise them on one stream.  Allocates nothing. */
+int pf_backward_noalloc(int precision, int dim, const int* n, const void* u_hat, void* u,
+                        void* stream);
+
 /* ---- operators on device arrays (math.py / space_solver.py kernels) ------
  * Arrays are device pointers of element type double (PF_FP64) or float
  * (PF_FP32); complex arrays interleaved.  shape = spatial extents of one

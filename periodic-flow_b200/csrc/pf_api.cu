@@ -67,6 +67,8 @@ static int fail(pf_solver* h, int code, const std::string& msg) {
   return code;
 }
 
+int pf::set_static_error(int code, const std::string& msg) { return fail(nullptr, code, msg); }
+
 #define PF_CUDA(h, call)                                                              \
   do {                                                                                \
     cudaError_t e_ = (call);                                                          \

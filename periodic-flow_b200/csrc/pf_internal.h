@@ -8,6 +8,9 @@
 
 namespace pf {
 
+// Record the message returned by pf_last_error(NULL); returns code.
+int set_static_error(int code, const std::string& msg);
+
 // kernel launch accounting: every launcher of this library reports here
 void count_launch();
 long long launch_total();

@@ -79,6 +79,8 @@ _SIGS = [
     ("pf_kernel_timer_read", C.c_int, [C.c_void_p, C.POINTER(C.c_double),
                                        C.POINTER(C.c_longlong)]),
     ("pf_launch_count", C.c_int, [C.POINTER(C.c_longlong)]),
+    ("pf_backward_noalloc", C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int), C.c_void_p,
+                                      C.c_void_p, C.c_void_p]),
     ("pf_op_cross", C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_longlong)] + [C.c_void_p] * 4),
     ("pf_op_curl", C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_longlong)] + [C.c_void_p] * 4),
     ("pf_op_apply_linear_operator", C.c_int,
