@@ -73,52 +73,47 @@ k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
   using C = cx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
+  // 32-bit offsets: every fused index space is below 2^31 for sides <= 512
   const int t = threadIdx.x, j = threadIdx.y;
-  const long long ncols = (long long)f.c1 * f.c2;
-  const long long q = (long long)blockIdx.x * T + t;
+  const int ncols = f.c1 * f.c2;
+  const int q = blockIdx.x * T + t;
   const bool active = q < ncols;
-  long long in_off = 0;
+  int in_off = 0;
   if (active) {
-    const int k1c = (int)(q / f.c2);
-    const int k2c = (int)(q - (long long)k1c * f.c2);
+    const int k1c = q / f.c2;
+    const int k2c = q - k1c * f.c2;
     const int i1 = k1c <= f.kmax1 ? k1c : k1c + (f.n1 - f.c1);
-    in_off = (long long)i1 * f.nh + k2c;
+    in_off = i1 * f.nh + k2c;
   }
-  const long long row_in = (long long)f.n1 * f.nh;
-  const long long fs_out = (long long)N * ncols;
+  const int row_in = f.n1 * f.nh;
+  const int fs_out = N * ncols;
+  const int fs_in = (int)f.nspec;
   auto smf = [&](int pos) -> C& { return sm[pos * T + t]; };
   auto sync = [] { __syncthreads(); };
-  R k0[E];
-  bool keep[E];
-#pragma unroll
-  for (int e = 0; e < E; ++e) {
-    const int kf = kfreq(j + G * e, N);
-    keep[e] = active && abs(kf) <= f.kmax0;
-    k0[e] = (R)(f.ks0 * kf);
-  }
+  // row e of the column: kept when |k0| <= kmax0 (recomputed, not stored)
+  auto kept = [&](int e) { return active && abs(kfreq(j + G * e, N)) <= f.kmax0; };
   C v[E], w[E];
 #pragma unroll
-  for (int e = 0; e < E; ++e)
-    v[e] = keep[e] ? uh[(long long)(j + G * e) * row_in + in_off] : czero<C>();
+  for (int e = 0; e < E; ++e) v[e] = kept(e) ? uh[(j + G * e) * row_in + in_off] : czero<C>();
   fft<N, E, +1>(v, j, tw, smf, sync);
   if (active) {
 #pragma unroll
-    for (int e = 0; e < E; ++e) A[(long long)(j + G * e) * ncols + q] = v[e];
+    for (int e = 0; e < E; ++e) A[(j + G * e) * ncols + q] = v[e];
   }
 #pragma unroll
   for (int c = 1; c <= 2; ++c) {
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-      v[e] = keep[e] ? uh[c * f.nspec + (long long)(j + G * e) * row_in + in_off] : czero<C>();
-      w[e] = cmuli(cscale(v[e], k0[e]));
+      v[e] = kept(e) ? uh[c * fs_in + (j + G * e) * row_in + in_off] : czero<C>();
+      w[e] = cmuli(cscale(v[e], (R)(f.ks0 * kfreq(j + G * e, N))));
     }
     fft<N, E, +1>(v, j, tw, smf, sync);
     fft<N, E, +1>(w, j, tw, smf, sync);
     if (active) {
 #pragma unroll
       for (int e = 0; e < E; ++e) {
-        A[c * fs_out + (long long)(j + G * e) * ncols + q] = v[e];
-        A[(2 + c) * fs_out + (long long)(j + G * e) * ncols + q] = w[e];
+        A[c * fs_out + (j + G * e) * ncols + q] = v[e];
+        A[(2 + c) * fs_out + (j + G * e) * ncols + q] = w[e];
       }
     }
   }
@@ -134,47 +129,44 @@ k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   const int t = threadIdx.x, j = threadIdx.y;
-  const long long ncols = (long long)f.n0 * f.c2;
-  const long long q = (long long)blockIdx.x * T + t;
+  const int ncols = f.n0 * f.c2;
+  const int q = blockIdx.x * T + t;
   const bool active = q < ncols;
-  long long in_base = 0, out_base = 0;
+  int in_base = 0, out_base = 0;
   R k2 = 0;
   if (active) {
-    const int x0 = (int)(q / f.c2);
-    const int k2c = (int)(q - (long long)x0 * f.c2);
-    in_base = (long long)x0 * f.c1 * f.c2 + k2c;
-    out_base = (long long)x0 * N * f.c2 + k2c;
+    const int x0 = q / f.c2;
+    const int k2c = q - x0 * f.c2;
+    in_base = x0 * f.c1 * f.c2 + k2c;
+    out_base = x0 * N * f.c2 + k2c;
     k2 = (R)(f.ks2 * k2c);
   }
-  const long long fs_in = (long long)f.n0 * f.c1 * f.c2;
-  const long long fs_out = (long long)f.n0 * N * f.c2;
+  const int fs_in = f.n0 * f.c1 * f.c2;
+  const int fs_out = f.n0 * N * f.c2;
   auto smf = [&](int pos) -> C& { return sm[pos * T + t]; };
   auto sync = [] { __syncthreads(); };
-  R k1[E];
-  long long in_off[E];
-  bool keep[E];
-#pragma unroll
-  for (int e = 0; e < E; ++e) {
+  // per element e of the line (recomputed, not stored): kept flag, k1,
+  // offset of the compact input index
+  auto kept = [&](int e) { return active && abs(kfreq(j + G * e, N)) <= f.kmax1; };
+  auto k1 = [&](int e) { return (R)(f.ks1 * kfreq(j + G * e, N)); };
+  auto off = [&](int e) {
     const int i1 = j + G * e;
-    const int kf = kfreq(i1, N);
-    keep[e] = active && abs(kf) <= f.kmax1;
-    k1[e] = (R)(f.ks1 * kf);
-    const int k1c = i1 <= f.kmax1 ? i1 : i1 - (N - f.c1);
-    in_off[e] = in_base + (long long)k1c * f.c2;
-  }
+    return in_base + (i1 <= f.kmax1 ? i1 : i1 - (N - f.c1)) * f.c2;
+  };
   auto store = [&](int fld, const C (&v)[E]) {
     if (active) {
 #pragma unroll
-      for (int e = 0; e < E; ++e) B[fld * fs_out + out_base + (long long)(j + G * e) * f.c2] = v[e];
+      for (int e = 0; e < E; ++e) B[fld * fs_out + out_base + (j + G * e) * f.c2] = v[e];
     }
   };
   C a[E], b[E], w[E];
   // omega0 = i (k1 u2 - k2 u1); u1; u2
 #pragma unroll
   for (int e = 0; e < E; ++e) {
-    a[e] = keep[e] ? A[1 * fs_in + in_off[e]] : czero<C>();
-    b[e] = keep[e] ? A[2 * fs_in + in_off[e]] : czero<C>();
-    w[e] = cmuli(csub(cscale(b[e], k1[e]), cscale(a[e], k2)));
+    const bool kp = kept(e);
+    a[e] = kp ? A[1 * fs_in + off(e)] : czero<C>();
+    b[e] = kp ? A[2 * fs_in + off(e)] : czero<C>();
+    w[e] = cmuli(csub(cscale(b[e], k1(e)), cscale(a[e], k2)));
   }
   fft<N, E, +1>(w, j, tw, smf, sync);
   store(3, w);
@@ -185,15 +177,16 @@ k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
   // omega2 = D1 - i k1 u0; omega1 = i k2 u0 - D2; u0
 #pragma unroll
   for (int e = 0; e < E; ++e) {
-    a[e] = keep[e] ? A[0 * fs_in + in_off[e]] : czero<C>();
-    b[e] = keep[e] ? A[3 * fs_in + in_off[e]] : czero<C>();
-    w[e] = csub(b[e], cmuli(cscale(a[e], k1[e])));
+    const bool kp = kept(e);
+    a[e] = kp ? A[0 * fs_in + off(e)] : czero<C>();
+    b[e] = kp ? A[3 * fs_in + off(e)] : czero<C>();
+    w[e] = csub(b[e], cmuli(cscale(a[e], k1(e))));
   }
   fft<N, E, +1>(w, j, tw, smf, sync);
   store(5, w);
 #pragma unroll
   for (int e = 0; e < E; ++e) {
-    b[e] = keep[e] ? A[4 * fs_in + in_off[e]] : czero<C>();
+    b[e] = kept(e) ? A[4 * fs_in + off(e)] : czero<C>();
     w[e] = csub(cmuli(cscale(a[e], k2)), b[e]);
   }
   fft<N, E, +1>(w, j, tw, smf, sync);
@@ -371,7 +364,7 @@ k_p4(cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
 // phase holds only a chunk of modes in registers; u_hat / u0 of a chunk are
 // loaded before any of its stores.
 template <typename R, int N, int NC, bool NOISE>
-__global__ void __launch_bounds__(TuneU<N>::T * TuneU<N>::G)
+__global__ void __launch_bounds__(TuneU<N>::T * TuneU<N>::G, 2)
 k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
   constexpr int E = TuneU<N>::E, G = TuneU<N>::G, T = TuneU<N>::T;
   constexpr int CH = E < 4 ? E : 4;
@@ -382,15 +375,23 @@ k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restr
   const int ncols = f.n1 * f.nh;
   const int q = blockIdx.x * T + t;
   const bool active = q < ncols;
+  const int fs = (int)f.nspec;
   auto sync = [] { __syncthreads(); };
-#pragma unroll 1
+  // component c + 1 is loaded while component c is transformed
+  C v[E], nx[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) nx[e] = active ? nl[(j + G * e) * ncols + q] : czero<C>();
+#pragma unroll
   for (int c = 0; c < 3; ++c) {
     C* Sc = S + c * N * T;
     auto smf = [&](int pos) -> C& { return Sc[pos * T + t]; };
-    C v[E];
 #pragma unroll
-    for (int e = 0; e < E; ++e)
-      v[e] = active ? nl[c * f.nspec + (long long)(j + G * e) * ncols + q] : czero<C>();
+    for (int e = 0; e < E; ++e) v[e] = nx[e];
+    if (c < 2) {
+#pragma unroll
+      for (int e = 0; e < E; ++e)
+        nx[e] = active ? nl[(c + 1) * fs + (j + G * e) * ncols + q] : czero<C>();
+    }
     fft<N, E, -1>(v, j, tw, smf, sync);
 #pragma unroll
     for (int e = 0; e < E; ++e) Sc[(j + G * e) * T + t] = v[e];
