@@ -215,6 +215,9 @@ def run_ours(args, dist, rank, world):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(n, args.cpu_steps)
+    ensemble = None
+    if rank == 0 and not args.no_ensemble:
+        ensemble = run_ensemble(args)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -229,7 +232,7 @@ def run_ours(args, dist, rank, world):
                        "dt_after_run": dt_now},
             "gpu_launches": int(c1.value - c0.value),
             "clocks": ck, "roofline": roofline, "step_roofline": step_roof,
-            "e2e": e2e, "cpu_baseline": cpu,
+            "e2e": e2e, "cpu_baseline": cpu, "batched": ensemble,
         }
         print(json.dumps(line), flush=True)
 
@@ -273,6 +276,94 @@ def run_e2e(args, uh0, rank, dist):
             "h2d_bytes_per_step": state_b / K, "d2h_bytes_per_step": (state_b + 16 * K) / K,
             "note": "per step: pf_step(1) + E,Z read-back (16 B); state up/download "
                     "(complex128) amortised over the steps; wall clock"}
+
+
+def ensemble_members(scale=1.0, precision="fp32"):
+    """Configuration 4: 128 x 128^2 + 32 x 256^2 (2D) + 8 x 64^3 (3D) correlated
+    fluctuating Stokes realisations, C(k) = exp(-(k/8)^2), seeds 0..167,
+    implicit predictor-corrector, dt = 0.02 (nu = 0.1, kT = 1e-3)."""
+    import math
+    from periodicflow import simulation as sim
+    sizes = ([(128, 128)] * max(1, int(128 * scale)) + [(256, 256)] * max(1, int(32 * scale))
+             + [(64, 64, 64)] * max(1, int(8 * scale)))
+    nu, kT = 0.1, 1e-3
+    out = []
+    for seed, N in enumerate(sizes):
+        s = sim.Solver(list(N), 0.02, 1.0, is_nonlinear=False, time_integrator="implicit_pc",
+                       viscosity=nu, noise_type="correlated", noise_mag=math.sqrt(2 * nu * kT),
+                       dealias="2/3", precision=precision, seed=seed)
+        s.set_correlation_function(np.exp(-s.space_solver.k2 / 64.0))
+        out.append(s)
+    return out
+
+
+def run_ensemble(args):
+    """Batched (one graph-captured launch for all realisations and steps) vs
+    the plain path: the same realisations solved one at a time (Solver.solve
+    per realisation; and a per-step loop, pf_step(1) per step, on a sample)."""
+    import torch
+    from periodicflow.ensemble import Ensemble
+    steps = args.ens_steps
+    plain = ensemble_members(args.ens_scale)
+    batch = ensemble_members(args.ens_scale)
+    pts = sum(int(np.prod(s.space_solver.N)) for s in plain)
+    nreal = len(plain)
+    torch.cuda.synchronize()
+    # plain, whole solves one after the other
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for s in plain:
+        s.space_solver.step(steps)
+    e1.record()
+    torch.cuda.synchronize()
+    plain_s = e0.elapsed_time(e1) / 1e3
+    probe = (0, nreal // 2, nreal - 1)
+    plain_states = {i: plain[i].space_solver.u_hat for i in probe}
+    # plain, stepwise loop (one time step per call) on a sample of steps
+    samp = min(steps, args.ens_stepwise_sample)
+    t0 = time.perf_counter()
+    for s in plain:
+        for _ in range(samp):
+            s.space_solver.step(1)
+    torch.cuda.synchronize()
+    stepwise_s = (time.perf_counter() - t0) * steps / samp
+    # batched: capture once, replay once
+    ens = Ensemble(batch)
+    ens.capture(steps)
+    torch.cuda.synchronize()
+    e0.record(ens._stream)
+    ens.replay()
+    e1.record(ens._stream)
+    ens.synchronize()
+    batch_s = e0.elapsed_time(e1) / 1e3
+    check = max(float(np.linalg.norm(batch[i].space_solver.u_hat - plain_states[i])
+                      / np.linalg.norm(plain_states[i])) for i in probe)
+    return {"workload": f"{nreal} correlated-noise Stokes realisations (2D 128^2, 2D 256^2, "
+                        f"3D 64^3), implicit PC, {steps} steps",
+            "realisations": nreal, "steps": steps,
+            "batched_s": batch_s, "plain_s": plain_s, "plain_stepwise_s_est": stepwise_s,
+            "batched_realisation_steps_per_s": nreal * steps / batch_s,
+            "plain_realisation_steps_per_s": nreal * steps / plain_s,
+            "batched_mpts_steps_per_s": pts * steps / 1e6 / batch_s,
+            "plain_mpts_steps_per_s": pts * steps / 1e6 / plain_s,
+            "speedup_vs_plain": plain_s / batch_s, "speedup_vs_stepwise": stepwise_s / batch_s,
+            "max_rel_diff_batched_vs_plain": check,
+            "stepwise_sample_steps": samp}
+
+
+def run_serving(args):
+    from periodicflow.serving import Server, poisson_requests
+    reqs = poisson_requests(args.serve_requests, rate=50.0, seed=2,
+                            max_steps=args.serve_max_steps)
+    srv = Server(hbm_budget=150e9)
+    cont = srv.run(reqs, "continuous")
+    ser = srv.run(reqs, "serial")
+    return {"workload": f"{len(reqs)} Poisson requests (50/s, seed 2): 2D 64^2-1024^2 and 3D "
+                        f"32^3-128^3 log-uniform, Taylor-Green or thermal noise, "
+                        f"100-{args.serve_max_steps} steps, 150 GB budget",
+            "continuous": cont, "serial": ser,
+            "throughput_ratio": cont["mpts_steps_per_s"] / ser["mpts_steps_per_s"],
+            "p99_ratio": ser["p99_latency_s"] / cont["p99_latency_s"]}
 
 
 def cpu_baseline(n, steps):
@@ -347,7 +438,20 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--ref-budget-s", type=float, default=120.0)
+    ap.add_argument("--mode", choices=["headline", "ensemble", "serving"], default="headline")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--ens-steps", type=int, default=5000)
+    ap.add_argument("--ens-scale", type=float, default=1.0)
+    ap.add_argument("--ens-stepwise-sample", type=int, default=50)
+    ap.add_argument("--serve-requests", type=int, default=60)
+    ap.add_argument("--serve-max-steps", type=int, default=5000)
     args = ap.parse_args()
+    if args.mode in ("ensemble", "serving"):
+        import torch
+        torch.cuda.set_device(0)
+        out = run_ensemble(args) if args.mode == "ensemble" else run_serving(args)
+        print(json.dumps({"mode": args.mode, **out}), flush=True)
+        return
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))
         rank = int(os.environ.get("RANK", "0"))

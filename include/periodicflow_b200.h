@@ -88,6 +88,8 @@ int pf_config_default(pf_config* cfg);
 
 /* Create a solver on the current CUDA device; state is zero. */
 int pf_create(const pf_config* cfg, pf_solver** out);
+/* Device bytes pf_create allocates for cfg (admission control; no device use). */
+int pf_footprint(const pf_config* cfg, unsigned long long* bytes);
 int pf_destroy(pf_solver* h);
 /* Order the handle's work on this cudaStream_t (NULL = legacy default). */
 int pf_set_stream(pf_solver* h, void* stream);
@@ -123,6 +125,11 @@ int pf_inject_noise(pf_solver* h, const double* w1, const double* w2, int where)
 
 /* Advance nsteps full time steps (all stages) on the device. */
 int pf_step(pf_solver* h, int nsteps);
+/* Capture "advance nsteps" as a CUDA graph on the handle's (non-default)
+ * stream; pf_graph_replay launches it with one call.  Noise-free solvers only
+ * (the noise step counter is a launch argument), without history recording. */
+int pf_graph_capture(pf_solver* h, int nsteps);
+int pf_graph_replay(pf_solver* h);
 
 /* Time, step counter and current dt (synchronises the stream). */
 int pf_get_time(pf_solver* h, double* t, long long* step, double* dt);
@@ -156,6 +163,27 @@ int pf_kernel_timer(pf_solver* h, int pass);
 int pf_kernel_timer_read(pf_solver* h, double* total_ms, long long* launches);
 /* Total kernels launched by this library in this process. */
 int pf_launch_count(long long* count);
+
+/* ---- ensembles of linear boxes -------------------------------------------
+ * No single reference counterpart: the reference runs one realisation per
+ * mpirun (simulation.py:189-225).  A batch advances many independent linear
+ * solvers (is_nonlinear = 0, no forcing, fixed dt, Philox or no noise) of
+ * mixed sizes and dimensions with one kernel launch per call, each mode's
+ * state in registers for all stages and steps.  Members keep owning their
+ * state; they must share precision, integrator and noise type, and must be
+ * idle (no work queued on their own streams) while batch work runs. */
+typedef struct pf_batch pf_batch;
+int pf_batch_create(pf_solver* const* members, int count, pf_batch** out);
+int pf_batch_destroy(pf_batch* b);
+int pf_batch_set_stream(pf_batch* b, void* stream);
+const char* pf_batch_last_error(const pf_batch* b);
+/* Advance every member nsteps (synchronous). */
+int pf_batch_step(pf_batch* b, int nsteps);
+/* Capture "advance nsteps" into a CUDA graph on the batch stream (must be a
+ * non-default stream); pf_batch_replay launches it (asynchronous). */
+int pf_batch_capture(pf_batch* b, int nsteps);
+int pf_batch_replay(pf_batch* b);
+int pf_batch_sync(pf_batch* b);
 
 /* ---- backward transform without device allocation ----------------------
  * No counterpart in the reference: an addition for callers that cannot call

@@ -43,13 +43,19 @@ struct pf_solver {
   int tpass = -1;
   std::vector<cudaEvent_t> tev;
   size_t tused = 0;
+  // captured "advance graph_steps" (pf_graph_capture / pf_graph_replay)
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  int graph_steps = 0;
+  long long graph_launches = 0;
+  bool capturing = false;
   std::string err;
 };
 
 // record an event on the solver stream when `pass` is the timed pass; events
 // come in (begin, end) pairs around each launch of that pass
 static void tmark(pf_solver* h, int pass) {
-  if (h->tpass != pass) return;
+  if (h->tpass != pass || h->capturing) return;
   if (h->tused == h->tev.size()) {
     cudaEvent_t e;
     if (cudaEventCreate(&e) != cudaSuccess) return;
@@ -68,6 +74,31 @@ static int fail(pf_solver* h, int code, const std::string& msg) {
 }
 
 int pf::set_static_error(int code, const std::string& msg) { return fail(nullptr, code, msg); }
+
+// Read-only view of a solver for the ensemble batch (pf_batch.cu).
+pf::SolverView pf::solver_view(const pf_solver* h) {
+  SolverView v;
+  v.g = h->g;
+  v.prec = h->prec;
+  v.ncomp = h->ncomp;
+  v.integrator = h->cfg.integrator;
+  v.noise_type = h->cfg.noise_type;
+  v.noise_src = h->cfg.noise_mag == 0.0 ? 0 : (h->cfg.noise_source == PF_NOISE_SRC_INJECTED ? 2 : 1);
+  v.linear_only = !h->cfg.is_nonlinear && h->cfg.forcing_eps <= 0.0 && h->cfg.cfl <= 0.0;
+  v.uhat = h->uhat;
+  v.lop = h->lop;
+  v.corr = h->corr;
+  v.dscal = h->dscal;
+  v.nu = h->cfg.viscosity;
+  v.noise_mag = h->cfg.noise_mag;
+  v.noise_norm = 1.0 / std::sqrt((double)h->g.nphys) / std::sqrt(2.0 - 2.0 / h->d);
+  v.dt = h->cfg.dt;
+  v.seed = h->cfg.seed;
+  v.step = h->step;
+  return v;
+}
+
+void pf::solver_add_steps(pf_solver* h, long long n) { h->step += n; }
 
 #define PF_CUDA(h, call)                                                              \
   do {                                                                                \
@@ -350,6 +381,8 @@ static int step_stokes(pf_solver* h, int nsteps) {
   A.nsteps = nsteps;
   A.noise_src = noise_src(h);
   A.noise_type = h->cfg.noise_type;
+  // the implicit predictor's output is never read by the corrector here
+  A.first_stage = h->cfg.integrator == PF_IMPLICIT_PC ? 1 : 0;
   tmark(h, PF_PASS_STOKES);
   cudaError_t se = launch_stokes<R>(A, h->ncomp, h->st);
   tmark(h, PF_PASS_STOKES);
@@ -542,6 +575,8 @@ int pf_destroy(pf_solver* h) {
     if (p) cudaFree(p);
   if (h->fused) fused_destroy(h->fused);
   for (cudaEvent_t e : h->tev) cudaEventDestroy(e);
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  if (h->graph) cudaGraphDestroy(h->graph);
   delete h;
   return PF_OK;
 }
@@ -821,3 +856,88 @@ int pf_launch_count(long long* count) {
 }
 
 }  // extern "C"
+
+// Stage coefficients of an integrator (shared with the ensemble batch).
+pf::Scheme pf::scheme_for(int integrator) { return make_scheme(integrator); }
+
+template <typename R>
+static int capture_steps(pf_solver* h, int nsteps) {
+  const bool linear = !h->cfg.is_nonlinear && h->cfg.forcing_eps <= 0.0 && h->cfg.cfl <= 0.0;
+  if (linear) return step_stokes<R>(h, nsteps);
+  for (int i = 0; i < nsteps; ++i) {
+    int rc = step_generic<R>(h);
+    if (rc) return rc;
+  }
+  return PF_OK;
+}
+
+extern "C" int pf_graph_capture(pf_solver* h, int nsteps) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  if (nsteps <= 0) return fail(h, PF_ERR_INVALID, "pf_graph_capture: nsteps must be > 0");
+  if (!h->st)
+    return fail(h, PF_ERR_INVALID, "pf_graph_capture: set a non-default stream first (pf_set_stream)");
+  if (noise_src(h) != kNoiseNone)
+    return fail(h, PF_ERR_UNSUPPORTED,
+                "pf_graph_capture: noisy solvers cannot be captured (the noise step counter is a "
+                "launch argument); use pf_step");
+  if (h->record_hist)
+    return fail(h, PF_ERR_UNSUPPORTED, "pf_graph_capture: history recording is not captured");
+  if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+  if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+  const long long l0 = launch_total();
+  h->capturing = true;
+  cudaError_t e = cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal);
+  int rc = PF_OK;
+  if (e == cudaSuccess) {
+    rc = h->prec == PF_FP64 ? capture_steps<double>(h, nsteps) : capture_steps<float>(h, nsteps);
+    e = cudaStreamEndCapture(h->st, &h->graph);
+  }
+  h->capturing = false;
+  h->graph_launches = launch_total() - l0;
+  add_launches(-h->graph_launches);  // recorded, not launched
+  if (rc) return rc;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&h->gexec, h->graph, 0);
+  if (e != cudaSuccess)
+    return fail(h, PF_ERR_CUDA, std::string("pf_graph_capture: ") + cudaGetErrorString(e));
+  h->graph_steps = nsteps;
+  return PF_OK;
+}
+
+extern "C" int pf_graph_replay(pf_solver* h) {
+  if (!h || !h->gexec) return fail(h, PF_ERR_INVALID, "pf_graph_replay: nothing captured");
+  PF_CUDA(h, cudaGraphLaunch(h->gexec, h->st));
+  add_launches(h->graph_launches);
+  h->step += h->graph_steps;
+  return PF_OK;
+}
+
+extern "C" int pf_footprint(const pf_config* c, unsigned long long* bytes) {
+  if (!c || !bytes) return fail(nullptr, PF_ERR_INVALID, "pf_footprint: null argument");
+  int rc = validate(c);
+  if (rc) return rc;
+  const int d = c->dim;
+  long long nspec = 1, nphys = 1;
+  for (int a = 0; a < d; ++a) {
+    nspec *= (a == d - 1) ? (c->n[a] / 2 + 1) : c->n[a];
+    nphys *= c->n[a];
+  }
+  const unsigned long long rsz = c->precision == PF_FP64 ? 8 : 4, cb = 2 * rsz;
+  const int ncomp = c->noise_type == PF_NOISE_THERMAL ? d * d : d;
+  unsigned long long st64 = std::max((unsigned long long)(2 * d * nspec), (unsigned long long)(d * nphys));
+  st64 = std::max(st64, (unsigned long long)(4 * ncomp * nspec));
+  unsigned long long b = cb * d * nspec * 2 + cb * 3 * nspec + 8 * st64 + 8 * kScalCount + 8 +
+                         16 * kHist;
+  if (c->is_nonlinear) {
+    b += cb * d * nspec + rsz * d * nphys + rsz * (d == 3 ? 3 : 1) * nphys;
+    bool pow2 = d == 3 && c->precision == PF_FP32 && c->fused && c->n[2] <= 256;
+    for (int a = 0; pow2 && a < 3; ++a)
+      pow2 = c->n[a] >= 16 && c->n[a] <= 512 && (c->n[a] & (c->n[a] - 1)) == 0;
+    if (pow2) {
+      const unsigned long long k1 = (c->n[1] - 1) / 3, k2 = (c->n[2] - 1) / 3;
+      b += cb * (5ull * c->n[0] * (2 * k1 + 1) * (k2 + 1) + 6ull * c->n[0] * c->n[1] * (k2 + 1));
+    }
+  }
+  if (c->noise_mag != 0.0 && c->noise_source == PF_NOISE_SRC_INJECTED) b += cb * 2 * ncomp * nspec;
+  *bytes = b;
+  return PF_OK;
+}

@@ -11,8 +11,11 @@ namespace pf {
 // Record the message returned by pf_last_error(NULL); returns code.
 int set_static_error(int code, const std::string& msg);
 
+struct SolverView;
+
 // kernel launch accounting: every launcher of this library reports here
 void count_launch();
+void add_launches(long long n);
 long long launch_total();
 inline cudaError_t launched() {
   count_launch();

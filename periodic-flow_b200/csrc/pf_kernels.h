@@ -39,6 +39,21 @@ template <typename R> struct StokesArgs {
   double dt, nu, noise_mag, noise_norm;
   uint64_t seed, step0;
   int nsteps, noise_src, noise_type;
+  int first_stage;  // 1: skip a stage the next one never reads (implicit PC, linear)
+};
+
+// What the ensemble batch needs to know about a member solver.
+struct SolverView {
+  Geo g;
+  int prec, ncomp, integrator, noise_type, noise_src;
+  bool linear_only;  // no nonlinear term, forcing or adaptive dt
+  void* uhat;
+  const void* lop;
+  const void* corr;
+  double* dscal;
+  double nu, noise_mag, noise_norm, dt;
+  uint64_t seed;
+  long long step;
 };
 
 template <typename R> cudaError_t launch_update(const UpdateArgs<R>& A, int ncomp, cudaStream_t st);
@@ -60,4 +75,11 @@ template <typename R>
 cudaError_t launch_spectrum(const cx<R>* u, const Geo& g, double* out, int nbins, double kunit,
                             cudaStream_t st);
 
+}  // namespace pf
+
+struct pf_solver;
+namespace pf {
+SolverView solver_view(const ::pf_solver* h);
+void solver_add_steps(::pf_solver* h, long long n);
+Scheme scheme_for(int integrator);
 }  // namespace pf

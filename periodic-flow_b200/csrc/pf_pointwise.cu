@@ -59,10 +59,16 @@ __global__ void __launch_bounds__(kBlock) k_stokes(StokesArgs<R> A) {
     const R corr = A.corr ? A.corr[m] : R(0);
     const DrawSite site = draw_site(g, mk_.ix.i0, mk_.ix.i1, mk_.ix.i2);
     const R nf = mk_.k2 == R(0) ? R(0) : (R)A.noise_norm;
+    // A mode whose noise amplitude is exactly zero (k = 0, or a correlation
+    // function that vanishes there) gets xi = 0 whatever the draws are, and
+    // counter-based draws of other modes do not depend on it: skip them.
+    const bool philox = A.noise_src == kNoisePhilox && nf != R(0) &&
+                        (A.noise_type == kThermal || corr != R(0));
+    const bool noisy = philox || A.noise_src == kNoiseInjected;
     for (int s = 0; s < A.nsteps; ++s) {
       const uint64_t step = A.step0 + (uint64_t)s;
       C w1[NC], w2[NC];
-      if (A.noise_src == kNoisePhilox) {
+      if (philox) {
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
           w1[c] = cscale(draw_value<R>(site, c, A.seed, step), nf);
@@ -78,10 +84,12 @@ __global__ void __launch_bounds__(kBlock) k_stokes(StokesArgs<R> A) {
       C u0[D];
 #pragma unroll
       for (int a = 0; a < D; ++a) u0[a] = u[a];
-      for (int st = 0; st < A.scheme.nstages; ++st) {
+      // first_stage = 1 skips the implicit predictor, whose result the
+      // corrector never reads when there is no nonlinear term or forcing
+      for (int st = A.first_stage; st < A.scheme.nstages; ++st) {
         const StageCoef& cf = A.scheme.st[st];
         C xi[D];
-        if (A.noise_src != kNoiseNone) {
+        if (noisy) {
           noise_term<R, D, NC>(xi, w1, w2, (R)cf.a, A.noise_type, mk_.k, mk_.k2, corr,
                                (R)A.noise_mag);
         } else {

@@ -11,6 +11,7 @@ namespace pf {
 
 static std::atomic<long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void add_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 long long launch_total() { return g_launches.load(std::memory_order_relaxed); }
 
 static __device__ float2 g_tw_f32[kTwSize];

@@ -54,6 +54,7 @@ _SIGS = [
     ("pf_config_default", C.c_int, [C.POINTER(PfConfig)]),
     ("pf_create", C.c_int, [C.POINTER(PfConfig), C.POINTER(C.c_void_p)]),
     ("pf_destroy", C.c_int, [C.c_void_p]),
+    ("pf_footprint", C.c_int, [C.POINTER(PfConfig), C.POINTER(C.c_ulonglong)]),
     ("pf_set_stream", C.c_int, [C.c_void_p, C.c_void_p]),
     ("pf_last_error", C.c_char_p, [C.c_void_p]),
     ("pf_sizes", C.c_int, [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
@@ -68,6 +69,8 @@ _SIGS = [
     ("pf_set_correlation", C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     ("pf_inject_noise", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     ("pf_step", C.c_int, [C.c_void_p, C.c_int]),
+    ("pf_graph_capture", C.c_int, [C.c_void_p, C.c_int]),
+    ("pf_graph_replay", C.c_int, [C.c_void_p]),
     ("pf_get_time", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                               C.POINTER(C.c_double)]),
     ("pf_set_time", C.c_int, [C.c_void_p, C.c_double, C.c_longlong]),
@@ -81,6 +84,14 @@ _SIGS = [
     ("pf_launch_count", C.c_int, [C.POINTER(C.c_longlong)]),
     ("pf_backward_noalloc", C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int), C.c_void_p,
                                       C.c_void_p, C.c_void_p]),
+    ("pf_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]),
+    ("pf_batch_destroy", C.c_int, [C.c_void_p]),
+    ("pf_batch_set_stream", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pf_batch_last_error", C.c_char_p, [C.c_void_p]),
+    ("pf_batch_step", C.c_int, [C.c_void_p, C.c_int]),
+    ("pf_batch_capture", C.c_int, [C.c_void_p, C.c_int]),
+    ("pf_batch_replay", C.c_int, [C.c_void_p]),
+    ("pf_batch_sync", C.c_int, [C.c_void_p]),
     ("pf_op_cross", C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_longlong)] + [C.c_void_p] * 4),
     ("pf_op_curl", C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_longlong)] + [C.c_void_p] * 4),
     ("pf_op_apply_linear_operator", C.c_int,

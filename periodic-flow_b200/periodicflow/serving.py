@@ -1,0 +1,237 @@
+"""Continuous-batching request loop for many independent solves on one GPU.
+
+Requests (a grid, a kind of run, a number of steps) arrive over time.  The
+server admits a waiting request as soon as its device footprint fits the HBM
+budget and a slot is free, keeps its state on the device, and advances all
+admitted requests together in rounds:
+
+* linear requests (fluctuating Stokes) go through one ensemble launch per
+  round (``pf_batch_step``): all of them, of any size, in one kernel;
+* nonlinear requests (Taylor-Green) each run a chunk of steps on their own
+  CUDA stream, so their kernels overlap on the device;
+
+requests that finish leave at the end of the round, freeing memory and a
+slot for the next arrivals.  ``mode='serial'`` is the one-at-a-time baseline:
+each request is created, solved to the end and freed before the next starts.
+Latency = finish - arrival; throughput = points x steps over the makespan.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as N
+from .space_solver import build_config, device_footprint
+
+KINDS = ("tgv", "thermal")
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float       # seconds after the start of the run
+    kind: str            # 'tgv' (nonlinear Taylor-Green) or 'thermal' (fluctuating Stokes)
+    N: tuple
+    steps: int
+    seed: int = 0
+    admitted: float | None = None
+    finished: float | None = None
+    result: np.ndarray | None = field(default=None, repr=False)
+
+    @property
+    def linear(self) -> bool:
+        return self.kind == "thermal"
+
+    @property
+    def points(self) -> int:
+        return int(np.prod(self.N))
+
+
+# physical set-up of the two kinds of request.  Thermal runs use the implicit
+# predictor-corrector: the explicit one is unstable once nu |k|^2 dt > 2
+# (|k| > 14 at nu = 0.1, dt = 0.01), i.e. on every grid served here.
+TGV = dict(dt=0.005, integrator="rk4", nu=1 / 1600)
+THERMAL = dict(dt=0.01, integrator="implicit_pc", nu=0.1, kT=1e-3)
+
+
+def _integrator_id(name):
+    from .time_integrator import DICT_TIME_INTEGRATORS
+    return DICT_TIME_INTEGRATORS[name].native_id
+
+
+def request_config(r: Request, precision="fp32"):
+    d = len(r.N)
+    dom = [(0.0, 2 * np.pi)] * d
+    if r.linear:
+        mag = math.sqrt(2 * THERMAL["nu"] * THERMAL["kT"])
+        return build_config(r.N, dom, False, _integrator_id(THERMAL["integrator"]), THERMAL["nu"],
+                            "thermal", mag, False, precision, THERMAL["dt"], r.seed, "philox",
+                            None, None, True)
+    return build_config(r.N, dom, True, _integrator_id(TGV["integrator"]), TGV["nu"], "thermal",
+                        0.0, False, precision, TGV["dt"], r.seed, "philox", None, None, True)
+
+
+def make_solver(r: Request, precision="fp32"):
+    """Solver with the request's initial state (Taylor-Green velocity, or rest
+    for the thermal-noise runs)."""
+    from .simulation import Solver
+    d = len(r.N)
+    if r.linear:
+        s = Solver(list(r.N), THERMAL["dt"], 1.0, is_nonlinear=False,
+                   time_integrator=THERMAL["integrator"], viscosity=THERMAL["nu"],
+                   noise_type="thermal", noise_mag=math.sqrt(2 * THERMAL["nu"] * THERMAL["kT"]),
+                   dealias="2/3", precision=precision, seed=r.seed)
+        return s
+    s = Solver(list(r.N), TGV["dt"], 1.0, time_integrator=TGV["integrator"], viscosity=TGV["nu"],
+               dealias="2/3", precision=precision)
+    x = s.space_solver.x
+    u = np.zeros((d,) + tuple(r.N))
+    if d == 3:
+        u[0] = np.sin(x[0]) * np.cos(x[1]) * np.cos(x[2])
+        u[1] = -np.cos(x[0]) * np.sin(x[1]) * np.cos(x[2])
+    else:
+        u[0] = np.sin(x[0]) * np.cos(x[1])
+        u[1] = -np.cos(x[0]) * np.sin(x[1])
+    s.initialize(u)
+    return s
+
+
+def poisson_requests(n, rate=50.0, seed=2, min_steps=100, max_steps=5000,
+                     sizes2d=(64, 128, 256, 512, 1024), sizes3d=(32, 64, 128)):
+    """Poisson arrivals; grid sides log-uniform over the built sizes; steps
+    log-uniform in [min_steps, max_steps]; kinds and dimensions equally likely."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n):
+        t += rng.exponential(1.0 / rate)
+        d = 2 if rng.random() < 0.5 else 3
+        side = int(rng.choice(sizes2d if d == 2 else sizes3d))
+        kind = KINDS[int(rng.integers(0, 2))]
+        steps = int(round(math.exp(rng.uniform(math.log(min_steps), math.log(max_steps)))))
+        out.append(Request(i, t, kind, (side,) * d, steps, seed=1000 + i))
+    return out
+
+
+class Server:
+    def __init__(self, hbm_budget=150e9, max_slots=64, chunk_nonlinear=25, chunk_linear=500,
+                 precision="fp32", keep_results=False):
+        self.budget = float(hbm_budget)
+        self.max_slots = max_slots
+        self.chunk_nl = chunk_nonlinear
+        self.chunk_lin = chunk_linear
+        self.precision = precision
+        self.keep_results = keep_results
+
+    def footprint(self, r: Request) -> int:
+        return device_footprint(request_config(r, self.precision))
+
+    # ------------------------------------------------------------------ runs
+    def run(self, requests, mode="continuous"):
+        import torch
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        for r in reqs:
+            r.admitted = r.finished = None
+            r.result = None
+        if mode == "serial":
+            return self._run_serial(reqs, torch)
+        return self._run_continuous(reqs, torch)
+
+    def _finish(self, r, sol, t0):
+        if self.keep_results:
+            r.result = sol.space_solver.u_hat
+        r.finished = time.perf_counter() - t0
+
+    def _run_serial(self, reqs, torch):
+        t0 = time.perf_counter()
+        for r in reqs:
+            wait = r.arrival - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(wait)
+            r.admitted = time.perf_counter() - t0
+            sol = make_solver(r, self.precision)
+            sol.space_solver.step(r.steps)
+            torch.cuda.synchronize()
+            self._finish(r, sol, t0)
+            del sol
+        return self._metrics(reqs, "serial")
+
+    def _run_continuous(self, reqs, torch):
+        from .ensemble import Ensemble
+        t0 = time.perf_counter()
+        pending = list(reqs)
+        active = []        # (request, solver, remaining, footprint, stream)
+        used = 0
+        ens, ens_ids = None, ()
+        while pending or active:
+            now = time.perf_counter() - t0
+            while (pending and pending[0].arrival <= now and len(active) < self.max_slots):
+                r = pending[0]
+                fp = self.footprint(r)
+                if used + fp > self.budget and active:
+                    break  # wait for memory to free up
+                pending.pop(0)
+                r.admitted = time.perf_counter() - t0
+                sol = make_solver(r, self.precision)
+                stream = None
+                if not r.linear:
+                    # own stream; a chunk of steps captured once as a CUDA graph
+                    stream = torch.cuda.Stream()
+                    sol.space_solver.set_stream(stream)
+                    if r.steps >= self.chunk_nl:
+                        sol.space_solver.capture(self.chunk_nl)
+                active.append([r, sol, r.steps, fp, stream])
+                used += fp
+            if not active:
+                if pending:
+                    time.sleep(max(0.0, pending[0].arrival - (time.perf_counter() - t0)))
+                continue
+            torch.cuda.synchronize()  # set-up copies of new members are done
+            # nonlinear requests: a chunk each on its own stream (asynchronous)
+            for a in active:
+                if not a[0].linear:
+                    c = min(self.chunk_nl, a[2])
+                    if c == self.chunk_nl:
+                        a[1].space_solver.replay()
+                    else:
+                        a[1].space_solver.step(c)
+                    a[2] -= c
+            # linear requests: one ensemble launch for all of them
+            lin = [a for a in active if a[0].linear]
+            if lin:
+                ids = tuple(a[0].rid for a in lin)
+                if ids != ens_ids:
+                    ens = Ensemble([a[1] for a in lin])
+                    ens_ids = ids
+                c = min(self.chunk_lin, min(a[2] for a in lin))
+                ens.step(c)
+                for a in lin:
+                    a[2] -= c
+            torch.cuda.synchronize()
+            keep = []
+            for a in active:
+                if a[2] == 0:
+                    self._finish(a[0], a[1], t0)
+                    used -= a[3]
+                else:
+                    keep.append(a)
+            if len(keep) != len(active):
+                if any(a[0].linear for a in active if a not in keep):
+                    ens, ens_ids = None, ()
+                active = keep
+        return self._metrics(reqs, "continuous")
+
+    @staticmethod
+    def _metrics(reqs, mode):
+        lat = np.array([r.finished - r.arrival for r in reqs])
+        svc = np.array([r.finished - r.admitted for r in reqs])
+        span = max(r.finished for r in reqs) - min(r.arrival for r in reqs)
+        pts_steps = sum(r.points * r.steps for r in reqs)
+        steps = sum(r.steps for r in reqs)
+        return {"mode": mode, "requests": len(reqs), "p50_latency_s": float(np.percentile(lat, 50)),
+                "p99_latency_s": float(np.percentile(lat, 99)),
+                "mean_service_s": float(svc.mean()), "makespan_s": float(span),
+                "steps_per_s": steps / span, "mpts_steps_per_s": pts_steps / 1e6 / span}

@@ -18,6 +18,43 @@ from .basis import FourierSpace
 NOISE_SOURCES = ("philox", "numpy", "injected")
 
 
+def build_config(Ns, domain, is_nonlinear, integrator_id, viscosity, noise_type, noise_mag,
+                 mask_nyquist, precision, dt, seed, noise_source, forcing, cfl, fused):
+    """The pf_config of a solver (include/periodicflow_b200.h)."""
+    dim = len(Ns)
+    cfg = N.PfConfig()
+    N.lib().pf_config_default(C.byref(cfg))
+    cfg.dim = dim
+    for a in range(3):
+        cfg.n[a] = Ns[a] if a < dim else 1
+        lo, hi = domain[a] if a < dim else (0.0, 2 * np.pi)
+        cfg.domain[a][0] = lo
+        cfg.domain[a][1] = hi
+    cfg.is_nonlinear = int(bool(is_nonlinear))
+    cfg.integrator = integrator_id
+    cfg.viscosity = viscosity
+    cfg.noise_type = N.PF_NOISE_THERMAL if noise_type == "thermal" else N.PF_NOISE_CORRELATED
+    cfg.noise_mag = noise_mag
+    cfg.dealias = N.PF_DEALIAS_TRUNCATE
+    cfg.mask_nyquist = int(bool(mask_nyquist))
+    cfg.precision = N.PF_FP64 if precision == "fp64" else N.PF_FP32
+    cfg.dt = dt
+    cfg.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+    cfg.noise_source = N.PF_NOISE_SRC_PHILOX if noise_source == "philox" else N.PF_NOISE_SRC_INJECTED
+    if forcing is not None:
+        cfg.forcing_eps, cfg.forcing_kf = float(forcing[0]), float(forcing[1])
+    cfg.cfl = float(cfl) if cfl else 0.0
+    cfg.fused = int(bool(fused))
+    return cfg
+
+
+def device_footprint(cfg) -> int:
+    """Device bytes a solver with this config allocates (no device use)."""
+    b = C.c_ulonglong()
+    N.check(N.lib().pf_footprint(C.byref(cfg), C.byref(b)), None, "pf_footprint")
+    return int(b.value)
+
+
 class SpaceSolver(FourierSpace):
     def __init__(self, comm, mpi_rank, N_, is_nonlinear: bool = True, viscosity: float = 1e-3,
                  noise_type: str = "thermal", noise_mag: float = 0.0, *, dt: float = 1e-3,
@@ -52,29 +89,9 @@ class SpaceSolver(FourierSpace):
         self.linear_operator = -viscosity * self.k2
         self.correlation_func = np.zeros(self.shape_spectral)
         self.forcing_cfg = forcing
-        cfg = N.PfConfig()
-        N.lib().pf_config_default(C.byref(cfg))
-        cfg.dim = self.dim
-        for a in range(3):
-            cfg.n[a] = self.N[a] if a < self.dim else 1
-            lo, hi = self.domain[a] if a < self.dim else (0.0, 2 * np.pi)
-            cfg.domain[a][0] = lo
-            cfg.domain[a][1] = hi
-        cfg.is_nonlinear = int(bool(is_nonlinear))
-        cfg.integrator = integrator_id
-        cfg.viscosity = viscosity
-        cfg.noise_type = N.PF_NOISE_THERMAL if noise_type == "thermal" else N.PF_NOISE_CORRELATED
-        cfg.noise_mag = noise_mag
-        cfg.dealias = N.PF_DEALIAS_TRUNCATE
-        cfg.mask_nyquist = int(self.nyquist_mask is not None)
-        cfg.precision = N.PF_FP64 if precision == "fp64" else N.PF_FP32
-        cfg.dt = dt
-        cfg.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
-        cfg.noise_source = N.PF_NOISE_SRC_PHILOX if noise_source == "philox" else N.PF_NOISE_SRC_INJECTED
-        if forcing is not None:
-            cfg.forcing_eps, cfg.forcing_kf = float(forcing[0]), float(forcing[1])
-        cfg.cfl = float(cfl) if cfl else 0.0
-        cfg.fused = int(bool(fused))
+        cfg = build_config(self.N, self.domain, is_nonlinear, integrator_id, viscosity,
+                           noise_type, noise_mag, self.nyquist_mask is not None, precision, dt,
+                           seed, noise_source, forcing, cfl, fused)
         h = C.c_void_p()
         N.check(N.lib().pf_create(C.byref(cfg), C.byref(h)), None, "pf_create")
         self._h = h
@@ -199,6 +216,25 @@ class SpaceSolver(FourierSpace):
 
     def step(self, nsteps: int):
         N.check(N.lib().pf_step(self._h, int(nsteps)), self._h, "step")
+
+    def set_stream(self, stream):
+        """Order this solver's device work on ``stream`` (torch.cuda.Stream,
+        raw cudaStream_t as int, or None for the legacy default stream)."""
+        ptr = getattr(stream, "cuda_stream", stream)
+        N.check(N.lib().pf_set_stream(self._h, C.c_void_p(ptr) if ptr else None), self._h,
+                "set_stream")
+
+    def footprint(self) -> int:
+        return device_footprint(self._cfg)
+
+    def capture(self, nsteps: int):
+        """Record "advance ``nsteps``" as a CUDA graph (needs a stream set with
+        set_stream and a noise-free run); replay() then costs one launch."""
+        N.check(N.lib().pf_graph_capture(self._h, int(nsteps)), self._h, "graph capture")
+        self._graph_steps = int(nsteps)
+
+    def replay(self):
+        N.check(N.lib().pf_graph_replay(self._h), self._h, "graph replay")
 
     def time(self):
         t, s, dt = C.c_double(), C.c_longlong(), C.c_double()

@@ -1,0 +1,124 @@
+"""Ensembles (one launch for many linear boxes) and the continuous-batching
+server: every result equals the same solve run alone."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+KT, NU = 1e-3, 0.1
+
+
+def stokes(N, seed, integ="implicit_pc", noise_type="thermal", precision="fp32", C=None,
+           dt=0.02):
+    """Explicit schemes need nu |k|^2 dt below their stability limit (~2)."""
+    from periodicflow import simulation as sim
+    s = sim.Solver(list(N), dt, 1.0, is_nonlinear=False, time_integrator=integ, viscosity=NU,
+                   noise_type=noise_type, noise_mag=math.sqrt(2 * NU * KT), dealias="2/3",
+                   precision=precision, seed=seed)
+    if C is not None:
+        s.set_correlation_function(C)
+    return s
+
+
+@pytest.mark.parametrize("precision,integ,dt", [("fp32", "implicit_pc", 0.02),
+                                               ("fp64", "implicit_pc", 0.02),
+                                               ("fp32", "explicit_pc", 0.001),
+                                               ("fp64", "rk3", 0.001)])
+def test_ensemble_equals_individual_solves(precision, integ, dt):
+    from periodicflow.ensemble import Ensemble
+    sizes = [(64, 64), (128, 128), (32, 32, 32), (128, 128), (16, 16, 16)]
+    a = [stokes(N, 10 + i, integ, precision=precision, dt=dt) for i, N in enumerate(sizes)]
+    b = [stokes(N, 10 + i, integ, precision=precision, dt=dt) for i, N in enumerate(sizes)]
+    ens = Ensemble(a)
+    ens.step(40)
+    ens.step(10)
+    for s in b:
+        s.space_solver.step(50)
+    for x, y in zip(a, b):
+        assert rel_l2(x.space_solver.u_hat, y.space_solver.u_hat) < 1e-6
+        tx, sx, _ = x.space_solver.time()
+        ty, sy, _ = y.space_solver.time()
+        assert sx == sy == 50 and tx == ty
+
+
+def test_ensemble_graph_replay_and_correlated_noise():
+    from periodicflow.ensemble import Ensemble
+    sizes = [(128, 128), (256, 256), (64, 64, 64)]
+    Cs = [np.exp(-O.Grid(N).k2 / 64.0) for N in sizes]  # exp(-(k/8)^2)
+    a = [stokes(N, i, "implicit_pc", "correlated", C=C) for i, (N, C) in enumerate(zip(sizes, Cs))]
+    b = [stokes(N, i, "implicit_pc", "correlated", C=C) for i, (N, C) in enumerate(zip(sizes, Cs))]
+    ens = Ensemble(a)
+    ens.capture(25)
+    for _ in range(3):
+        ens.replay()
+    ens.synchronize()
+    for s in b:
+        s.space_solver.step(75)
+    for x, y in zip(a, b):
+        assert rel_l2(x.space_solver.u_hat, y.space_solver.u_hat) < 1e-6
+        assert x.space_solver.time()[1] == 75 and x.step == 75
+
+
+@pytest.mark.parametrize("N", [(32, 32, 32), (64, 64)])
+def test_graph_replay_equals_stepping(N):
+    import torch
+    from periodicflow import simulation as sim
+    from periodicflow.serving import Request, make_solver
+    r = Request(0, 0.0, "tgv", N, 30)
+    a, b = make_solver(r), make_solver(r)
+    st = torch.cuda.Stream()
+    a.space_solver.set_stream(st)
+    a.space_solver.capture(10)
+    for _ in range(3):
+        a.space_solver.replay()
+    b.space_solver.step(30)
+    torch.cuda.synchronize()
+    assert rel_l2(a.space_solver.u_hat, b.space_solver.u_hat) == 0.0
+    assert a.space_solver.time()[1] == 30
+    noisy = stokes((32, 32), 1)
+    noisy.space_solver.set_stream(st)
+    with pytest.raises(NotImplementedError):
+        noisy.space_solver.capture(5)
+
+
+def test_ensemble_rejects_nonlinear_members():
+    from periodicflow import simulation as sim
+    from periodicflow.ensemble import Ensemble
+    s = sim.Solver([32, 32], 0.01, 1.0, dealias="2/3")
+    with pytest.raises(NotImplementedError):
+        Ensemble([s])
+
+
+def test_served_results_equal_alone():
+    from periodicflow.serving import Request, Server
+    reqs = [Request(0, 0.00, "thermal", (64, 64), 120, seed=1),
+            Request(1, 0.00, "tgv", (32, 32, 32), 60),
+            Request(2, 0.01, "thermal", (32, 32, 32), 90, seed=2),
+            Request(3, 0.02, "tgv", (64, 64), 80),
+            Request(4, 0.02, "thermal", (128, 128), 300, seed=3),
+            Request(5, 0.03, "tgv", (16, 16, 16), 40)]
+    srv = Server(chunk_nonlinear=15, chunk_linear=50, keep_results=True)
+    m = srv.run(reqs, "continuous")
+    mixed = {r.rid: r.result for r in reqs}
+    assert m["requests"] == 6 and m["p99_latency_s"] >= m["p50_latency_s"] > 0
+    srv.run(reqs, "serial")
+    for r in reqs:
+        assert rel_l2(mixed[r.rid], r.result) < 1e-6, r
+
+
+def test_admission_respects_budget():
+    from periodicflow.serving import Request, Server
+    reqs = [Request(i, 0.0, "thermal", (128, 128), 20, seed=i) for i in range(4)]
+    srv = Server(chunk_linear=10)
+    one = srv.footprint(reqs[0])
+    srv.budget = 2 * one  # at most two resident at a time
+    m = srv.run(reqs, "continuous")
+    assert m["requests"] == 4
+    admitted = sorted(r.admitted for r in reqs)
+    finished = sorted(r.finished for r in reqs)
+    assert admitted[2] >= finished[0]  # the third waited for memory
