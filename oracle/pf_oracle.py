@@ -140,10 +140,91 @@ class Grid:
         return sfft.irfftn(uh, s=self.N, axes=axes, workers=FFT_WORKERS) * self.prodN
 
     def backward_dealiased(self, uh):
-        """Vp.backward / Wp.backward of space_solver.py:284,291 for the 2/3 rule."""
+        """Vp.backward / Wp.backward of space_solver.py:284,291.
+
+        '2/3': backward of the truncated copy.  '3/2' (basis.py:133-134): the
+        spectrum padded onto M = 3N/2 per axis (Nyquist modes of even sides
+        split in half between +N/2 and -N/2; halved on the last axis), then the
+        unnormalised backward transform on the M grid.
+        """
         if self.dealias in ("2/3", "truncate"):
             return self.backward(uh * self.dealias_mask)
-        raise NotImplementedError("3/2 padding is not restated in the oracle")
+        M = self.padded_shape()
+        axes = tuple(range(-self.dim, 0))
+        return sfft.irfftn(self.pad(uh), s=M, axes=axes, workers=FFT_WORKERS) * float(np.prod(M))
+
+    def forward_dealiased(self, u):
+        """Vp.forward of space_solver.py:296: '2/3' plain forward; '3/2' forward
+        on the M grid (normalised by 1/prod M) folded back to the N grid."""
+        if self.dealias in ("2/3", "truncate"):
+            return self.forward(u)
+        M = self.padded_shape()
+        axes = tuple(range(-self.dim, 0))
+        return self.truncate(sfft.rfftn(u, axes=axes, workers=FFT_WORKERS) / float(np.prod(M)))
+
+    def padded_shape(self):
+        return [3 * n // 2 for n in self.N]
+
+    @staticmethod
+    def _sl(ndim, axis, lo, hi):
+        idx = [slice(None)] * ndim
+        idx[axis] = slice(lo, hi)
+        return tuple(idx)
+
+    def pad(self, uh):
+        """N-grid half spectrum (leading component axes allowed) -> M grid."""
+        out = np.asarray(uh)
+        nd = out.ndim
+        for ax in range(self.dim):
+            a = nd - self.dim + ax
+            N, M = self.N[ax], 3 * self.N[ax] // 2
+            h = N // 2
+            last = ax == self.dim - 1
+            shp = list(out.shape)
+            shp[a] = M // 2 + 1 if last else M
+            new = np.zeros(shp, dtype=np.complex128)
+            S = lambda lo, hi: self._sl(nd, a, lo, hi)  # noqa: E731
+            if last:
+                new[S(0, h)] = out[S(0, h)]
+                new[S(h, h + 1)] = (0.5 if N % 2 == 0 else 1.0) * out[S(h, h + 1)]
+            else:
+                new[S(0, h)] = out[S(0, h)]
+                new[S(M - h + 1, M)] = out[S(N - h + 1, N)]
+                new[S(h, h + 1)] = 0.5 * out[S(h, h + 1)]
+                new[S(M - h, M - h + 1)] = 0.5 * out[S(h, h + 1)]
+            out = new
+        return out
+
+    def truncate(self, P):
+        """M-grid half spectrum -> N grid: the last axis first (its Nyquist
+        entry gains the conjugate of the mirror mode, i.e. the -N/2 partner),
+        then every complex axis folds +N/2 and -N/2 into the Nyquist index."""
+        out = np.asarray(P)
+        nd = out.ndim
+        a = nd - 1
+        N = self.N[-1]
+        h = N // 2
+        out = out[self._sl(nd, a, 0, h + 1)].copy()
+        if N % 2 == 0:
+            nyq = out[self._sl(nd, a, h, h + 1)]
+            mir = nyq
+            for ax in range(self.dim - 1):
+                b = nd - self.dim + ax
+                mir = np.roll(np.flip(mir, axis=b), 1, axis=b)
+            out[self._sl(nd, a, h, h + 1)] = nyq + np.conj(mir)
+        for ax in range(self.dim - 1):
+            b = nd - self.dim + ax
+            N, M = self.N[ax], 3 * self.N[ax] // 2
+            h = N // 2
+            shp = list(out.shape)
+            shp[b] = N
+            new = np.zeros(shp, dtype=np.complex128)
+            S = lambda lo, hi: self._sl(nd, b, lo, hi)  # noqa: E731
+            new[S(0, h)] = out[S(0, h)]
+            new[S(N - h + 1, N)] = out[S(M - h + 1, M)]
+            new[S(h, h + 1)] = out[S(h, h + 1)] + out[S(M - h, M - h + 1)]
+            out = new
+        return out
 
 
 # ----------------------------------------------------------------------------
@@ -467,9 +548,8 @@ def linear_forcing(grid, uh, eps, kf):
 
 def cfl_dt(grid, uh, cfl):
     """dt = CFL / max_x sum_i |u_i| / dx_i on the dealiased physical field."""
-    u = grid.backward_dealiased(uh)
-    s = 0.0
-    acc = np.zeros(grid.phys_shape)
+    u = grid.backward_dealiased(uh)  # on the 3N/2 grid for the 3/2 rule
+    acc = np.zeros(u.shape[1:])
     for i in range(grid.dim):
         acc += np.abs(u[i]) / (grid.lengths[i] / grid.N[i])
     s = float(acc.max())
@@ -585,7 +665,7 @@ class OracleSolver:
         g = self.grid
         w = g.backward_dealiased(curl(g.k, uh))
         u = g.backward_dealiased(uh)
-        N = g.forward(cross(u, w))
+        N = g.forward_dealiased(cross(u, w))
         N, _ = leray_projection(N, g.k, g.k_over_k2)
         if g.nyquist_mask is not None:
             N = N * g.nyquist_mask

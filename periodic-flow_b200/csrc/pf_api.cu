@@ -24,6 +24,12 @@ struct pf_solver {
   void* spec_tmp = nullptr;  // 3 * nspec complex
   void* phys_u = nullptr; // d * nphys real
   void* phys_w = nullptr; // (3D: 3, 2D: 1) * nphys real
+  // 3/2 rule: padded grid M = 3N/2 and its work arrays
+  Geo gM;
+  bool padded = false;
+  void* specM = nullptr;    // 3 * nspec(M) complex
+  void* physM_u = nullptr;  // d * nphys(M) real
+  void* physM_w = nullptr;  // (3D: 3, 2D: 1) * nphys(M) real
   void* lop = nullptr;    // nspec real (user L)
   void* corr = nullptr;   // nspec real (user C)
   void* winj = nullptr;   // 2 * ncomp * nspec complex
@@ -154,8 +160,7 @@ static unsigned blocks_for(long long n) {
 
 // ------------------------------------------------------------ transforms
 template <typename R>
-static cudaError_t backward_inplace(pf_solver* h, cx<R>* X, R* P, int nc) {
-  const Geo& g = h->g;
+static cudaError_t backward_g(pf_solver* h, const Geo& g, cx<R>* X, R* P, int nc) {
   cudaError_t e;
   if (g.dim == 3) {
     const long long plane = (long long)g.s[1] * g.nh;
@@ -183,8 +188,12 @@ static cudaError_t backward_inplace(pf_solver* h, cx<R>* X, R* P, int nc) {
 }
 
 template <typename R>
-static cudaError_t forward_into(pf_solver* h, const R* P, cx<R>* X, int nc) {
-  const Geo& g = h->g;
+static cudaError_t backward_inplace(pf_solver* h, cx<R>* X, R* P, int nc) {
+  return backward_g<R>(h, h->g, X, P, nc);
+}
+
+template <typename R>
+static cudaError_t forward_g(pf_solver* h, const Geo& g, const R* P, cx<R>* X, int nc) {
   const double scale = 1.0 / (double)g.nphys;
   cudaError_t e;
   if (g.dim == 3) {
@@ -210,6 +219,43 @@ static cudaError_t forward_into(pf_solver* h, const R* P, cx<R>* X, int nc) {
   e = fft_strided<R>(X, g.n[0], -1, g.nh, nc, g.nspec, g.nh, 1.0, h->st);
   tmark(h, PF_PASS_FFT_STRIDED);
   return e;
+}
+
+template <typename R>
+static cudaError_t forward_into(pf_solver* h, const R* P, cx<R>* X, int nc) {
+  return forward_g<R>(h, h->g, P, X, nc);
+}
+
+// 3/2 rule (basis.py:133-134): u and omega = i k x u padded onto the M = 3N/2
+// grid, u x omega there, forward transform normalised by 1 / prod M, then
+// truncated back to the N grid, unprojected, into h->nl
+template <typename R>
+static cudaError_t nonlinear_padded(pf_solver* h, bool want_max) {
+  const Geo& g = h->g;
+  const Geo& gM = h->gM;
+  cx<R>* tmp = (cx<R>*)h->specM;
+  const int wc = g.dim == 3 ? 3 : 1;
+  cudaError_t e = launch_pad<R>(tmp, (const cx<R>*)h->uhat, g, gM, h->d, 1, h->st);
+  if (e != cudaSuccess) return e;
+  e = backward_g<R>(h, gM, tmp, (R*)h->physM_w, wc);
+  if (e != cudaSuccess) return e;
+  e = launch_pad<R>(tmp, (const cx<R>*)h->uhat, g, gM, h->d, 0, h->st);
+  if (e != cudaSuccess) return e;
+  e = backward_g<R>(h, gM, tmp, (R*)h->physM_u, h->d);
+  if (e != cudaSuccess) return e;
+  if (want_max) {
+    e = cudaMemsetAsync(h->maxbits, 0, sizeof(unsigned long long), h->st);
+    if (e != cudaSuccess) return e;
+  }
+  // iterate over the M grid, measure |u_i| / dx_i with the N-grid spacing
+  Geo gx = g;
+  gx.nphys = gM.nphys;
+  e = launch_cross<R>((R*)h->physM_u, (const R*)h->physM_w, gx, want_max ? h->maxbits : nullptr,
+                      h->st);
+  if (e != cudaSuccess) return e;
+  e = forward_g<R>(h, gM, (const R*)h->physM_u, tmp, h->d);
+  if (e != cudaSuccess) return e;
+  return launch_truncate<R>((cx<R>*)h->nl, tmp, g, gM, h->d, h->st);
 }
 
 // nonlinear term u x w (unprojected) of the current state into h->nl
@@ -312,7 +358,8 @@ static int step_generic(pf_solver* h) {
           PF_CUDA(h, fe);
         }
       } else {
-        PF_CUDA(h, nonlinear_generic<R>(h, s == 0 && cfl));
+        PF_CUDA(h, h->padded ? nonlinear_padded<R>(h, s == 0 && cfl)
+                             : nonlinear_generic<R>(h, s == 0 && cfl));
       }
       if (s == 0 && cfl) PF_CUDA(h, launch_set_dt(h->dscal, h->maxbits, h->cfg.cfl, h->st));
     } else if (s == 0 && cfl) {
@@ -496,8 +543,14 @@ static int validate(const pf_config* c) {
   if (c->noise_type != PF_NOISE_THERMAL && c->noise_type != PF_NOISE_CORRELATED)
     return fail(nullptr, PF_ERR_INVALID,
                 "Invalid noise type. Options are 'thermal' or 'correlated'.");
-  if (c->dealias != PF_DEALIAS_TRUNCATE)
-    return fail(nullptr, PF_ERR_UNSUPPORTED, "3/2 padding dealiasing is not built");
+  if (c->dealias != PF_DEALIAS_TRUNCATE && c->dealias != PF_DEALIAS_PAD)
+    return fail(nullptr, PF_ERR_INVALID, "FourierSpace: Invalid dealiasing rule.");
+  if (c->dealias == PF_DEALIAS_PAD && c->is_nonlinear) {
+    for (int a = 0; a < c->dim; ++a)
+      if (c->n[a] % 2 != 0 || !fft_length_supported(3 * c->n[a] / 2))
+        return fail(nullptr, PF_ERR_UNSUPPORTED,
+                    "3/2 padding needs a padded size 3n/2 with a built FFT (n = 8..512)");
+  }
   if (c->precision != PF_FP32 && c->precision != PF_FP64)
     return fail(nullptr, PF_ERR_INVALID, "precision must be PF_FP32 or PF_FP64");
   if (!(c->dt > 0.0)) return fail(nullptr, PF_ERR_INVALID, "dt must be positive");
@@ -547,7 +600,23 @@ int pf_create(const pf_config* cfg, pf_solver** out) {
             alloc((void**)&h->dscal, sizeof(double) * kScalCount) &&
             alloc((void**)&h->maxbits, sizeof(unsigned long long)) &&
             alloc((void**)&h->hist_dev, sizeof(double) * 2 * kHist);
-  if (ok && cfg->is_nonlinear) {
+  if (ok && cfg->is_nonlinear && cfg->dealias == PF_DEALIAS_PAD) {
+    h->padded = true;
+    Geo& gM = h->gM;
+    gM = g;
+    gM.nspec = 1;
+    gM.nphys = 1;
+    for (int a = 0; a < h->d; ++a) {
+      gM.n[a] = 3 * g.n[a] / 2;
+      gM.s[a] = gM.n[a];
+    }
+    gM.nh = gM.n[h->d - 1] / 2 + 1;
+    gM.s[h->d - 1] = gM.nh;
+    for (int a = 0; a < h->d; ++a) { gM.nspec *= gM.s[a]; gM.nphys *= gM.n[a]; }
+    ok = alloc(&h->nl, cb * h->d * g.nspec) && alloc(&h->specM, cb * 3 * gM.nspec) &&
+         alloc(&h->physM_u, h->rsz * h->d * gM.nphys) &&
+         alloc(&h->physM_w, h->rsz * wc * gM.nphys);
+  } else if (ok && cfg->is_nonlinear) {
     ok = alloc(&h->nl, cb * h->d * g.nspec) && alloc(&h->phys_u, h->rsz * h->d * g.nphys) &&
          alloc(&h->phys_w, h->rsz * wc * g.nphys);
   }
@@ -569,7 +638,8 @@ int pf_create(const pf_config* cfg, pf_solver** out) {
 
 int pf_destroy(pf_solver* h) {
   if (!h) return PF_OK;
-  void* ptrs[] = {h->uhat, h->u0, h->nl, h->spec_tmp, h->phys_u, h->phys_w, h->lop,
+  void* ptrs[] = {h->uhat, h->u0, h->nl, h->spec_tmp, h->phys_u, h->phys_w,
+                  h->specM, h->physM_u, h->physM_w, h->lop,
                   h->corr, h->winj, h->stage64, h->dscal, h->maxbits, h->hist_dev};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -927,7 +997,15 @@ extern "C" int pf_footprint(const pf_config* c, unsigned long long* bytes) {
   st64 = std::max(st64, (unsigned long long)(4 * ncomp * nspec));
   unsigned long long b = cb * d * nspec * 2 + cb * 3 * nspec + 8 * st64 + 8 * kScalCount + 8 +
                          16 * kHist;
-  if (c->is_nonlinear) {
+  if (c->is_nonlinear && c->dealias == PF_DEALIAS_PAD) {
+    unsigned long long msp = 1, mph = 1;
+    for (int a = 0; a < d; ++a) {
+      const int m = 3 * c->n[a] / 2;
+      msp *= (a == d - 1) ? (m / 2 + 1) : m;
+      mph *= m;
+    }
+    b += cb * d * nspec + cb * 3 * msp + rsz * d * mph + rsz * (d == 3 ? 3 : 1) * mph;
+  } else if (c->is_nonlinear) {
     b += cb * d * nspec + rsz * d * nphys + rsz * (d == 3 ? 3 : 1) * nphys;
     bool pow2 = d == 3 && c->precision == PF_FP32 && c->fused && c->n[2] <= 256;
     for (int a = 0; pow2 && a < 3; ++a)

@@ -20,8 +20,13 @@ namespace pf {
 // ---- twiddle tables ---------------------------------------------------------
 // A table for length N holds exp(-2 pi i m / N), m in [0, N), rounded from
 // FP64; kernels receive its device address (tables live in pf_tables.cu).
+// Lengths with tables: 2^b (2..1024) and 3 * 2^b (12..768).
 constexpr int kMaxFFT = 1024;
-constexpr int kTwSize = 2 * kMaxFFT - 2;
+constexpr int kMax3FFT = 768;
+constexpr int kTwPow2 = 2 * kMaxFFT - 2;        // sum of 2^b tables
+constexpr int kTwSize = kTwPow2 + 2 * kMax3FFT - 12;
+// offset of the table of length n (2^b: n - 2; 12 * 2^m: kTwPow2 + n - 12)
+PF_HD int tw_offset(int n) { return (n % 3 == 0) ? kTwPow2 + n - 12 : n - 2; }
 
 template <typename C> PF_D C ldtw(const C* p) { return __ldg(p); }
 
@@ -102,8 +107,26 @@ template <int DIR, typename C> PF_D void dft16(C* v) {
   }
 }
 
+// radix 3: W = exp(DIR 2 pi i / 3) = -1/2 + i DIR sqrt(3)/2
+template <int DIR, typename C> PF_D void dft3(C& a, C& b, C& c) {
+  using R = decltype(a.x);
+  const R s = R(DIR) * R(0.86602540378443864676);
+  const C t = cadd(b, c), d = csub(b, c);
+  C m;  // a - t/2
+  m.x = a.x - R(0.5) * t.x;
+  m.y = a.y - R(0.5) * t.y;
+  a = cadd(a, t);
+  C sd;  // i s d
+  sd.x = -s * d.y;
+  sd.y = s * d.x;
+  b = cadd(m, sd);
+  c = csub(m, sd);
+}
+
 template <int R, int DIR, typename C> PF_D void dft(C* v) {
   if constexpr (R == 1) {
+  } else if constexpr (R == 3) {
+    dft3<DIR>(v[0], v[1], v[2]);
   } else if constexpr (R == 2) {
     dft2<DIR>(v[0], v[1]);
   } else if constexpr (R == 4) {
@@ -117,11 +140,18 @@ template <int R, int DIR, typename C> PF_D void dft(C* v) {
 }
 
 // ---- stage plan -------------------------------------------------------------
-// Greedy radices: E, E, ..., remainder.  Ns(s) = product of earlier radices.
+// N = 2^b or 3 * 2^b.  A factor 3 is done first as a radix-3 stage (E must
+// then be a multiple of 3); the power-of-two part takes greedy radices E2,
+// E2, ..., remainder with E2 the power-of-two part of E.  Ns(s) = product of
+// earlier radices.  Every radix divides E.
 template <int N, int E> struct Plan {
+  static constexpr int P3 = (N % 3 == 0) ? 1 : 0;
+  static constexpr int E2 = (E % 3 == 0) ? E / 3 : E;
+  static_assert(!P3 || E % 3 == 0, "a radix-3 stage needs E divisible by 3");
   static constexpr int radix(int s) {
-    int rem = N, r = 1;
-    for (int t = 0; t <= s; ++t) { r = rem < E ? rem : E; rem /= r; }
+    if (P3 && s == 0) return 3;
+    int rem = P3 ? N / 3 : N, r = 1;
+    for (int t = P3; t <= s; ++t) { r = rem < E2 ? rem : E2; rem /= r; }
     return r;
   }
   static constexpr int ns(int s) {

@@ -13,7 +13,10 @@
 namespace pf {
 
 template <int N> struct Tune {
-  static constexpr int E = N <= 16 ? N : (N <= 64 ? 8 : 16);
+  // powers of two: 8 or 16 values per thread; 3 * 2^b: 12 or 24 (a radix-3
+  // stage needs E divisible by 3)
+  static constexpr int E = (N % 3 == 0) ? (N <= 24 ? N : (N <= 96 ? 12 : 24))
+                                        : (N <= 16 ? N : (N <= 64 ? 8 : 16));
   static constexpr int G = N / E;
   static constexpr int T = (256 / G) < 4 ? 4 : ((256 / G) > 64 ? 64 : 256 / G);
   static constexpr int L = (128 / G) < 1 ? 1 : 128 / G;  // line pairs per CTA
@@ -135,7 +138,7 @@ k_r2c_last(const R* __restrict__ in, cx<R>* __restrict__ out, long long nlines,
     const int k = j + G * e;
     if (k <= H) {
       const C zk = smf(k);
-      const C zn = smf((N - k) & (N - 1));
+      const C zn = smf(k == 0 ? 0 : N - k);
       C A, Bv;
       A.x = (zk.x + zn.x) * h; A.y = (zk.y - zn.y) * h;
       // (zk - conj zn) / 2i
@@ -159,12 +162,14 @@ static cudaError_t launch_strided(cx<R>* data, int dir, long long ncols, long lo
   using TN = Tune<N>;
   const cx<R>* twb = tw_base<R>();
   if (!twb) return cudaErrorNotReady;  // tables not built on this device
-  const cx<R>* tw = twb + (N - 2);
+  const cx<R>* tw = twb + tw_offset(N);
   const long long ntotal = ncols * nplanes;
   if (ntotal == 0) return cudaSuccess;
   dim3 block(TN::T, TN::G);
   dim3 grid((unsigned)((ntotal + TN::T - 1) / TN::T));
-  size_t sm = TN::G > 1 ? sizeof(cx<R>) * N * TN::T : 0;
+  // exchange buffer whenever the plan has more than one stage (a 3 * 2^b
+  // length with one thread per line still exchanges between its stages)
+  size_t sm = Plan<N, TN::E>::stages() > 1 ? sizeof(cx<R>) * N * TN::T : 0;
   const int us = scale != 1.0;
   cudaError_t e;
   if (dir < 0) {
@@ -185,7 +190,7 @@ static cudaError_t launch_c2r(const cx<R>* in, R* out, long long nlines, long lo
   using TN = Tune<N>;
   const cx<R>* twb = tw_base<R>();
   if (!twb) return cudaErrorNotReady;  // tables not built on this device
-  const cx<R>* tw = twb + (N - 2);
+  const cx<R>* tw = twb + tw_offset(N);
   const long long npairs = (nlines + 1) / 2;
   if (npairs == 0) return cudaSuccess;
   dim3 block(TN::G, TN::L);
@@ -203,7 +208,7 @@ static cudaError_t launch_r2c(const R* in, cx<R>* out, long long nlines, long lo
   using TN = Tune<N>;
   const cx<R>* twb = tw_base<R>();
   if (!twb) return cudaErrorNotReady;  // tables not built on this device
-  const cx<R>* tw = twb + (N - 2);
+  const cx<R>* tw = twb + tw_offset(N);
   const long long npairs = (nlines + 1) / 2;
   if (npairs == 0) return cudaSuccess;
   dim3 block(TN::G, TN::L);
@@ -216,7 +221,10 @@ static cudaError_t launch_r2c(const R* in, cx<R>* out, long long nlines, long lo
 }
 
 bool fft_length_supported(int n) {
-  return n >= 4 && n <= kMaxFFT && (n & (n - 1)) == 0;
+  if (n >= 4 && n <= kMaxFFT && (n & (n - 1)) == 0) return true;
+  if (n % 3 != 0) return false;
+  const int m = n / 3;  // 3 * 2^b, 12..768
+  return n >= 12 && n <= kMax3FFT && (m & (m - 1)) == 0;
 }
 
 #define PF_SWITCH_N(n, CALL)                     \
@@ -230,6 +238,13 @@ bool fft_length_supported(int n) {
     case 256: return CALL(256);                  \
     case 512: return CALL(512);                  \
     case 1024: return CALL(1024);                \
+    case 12: return CALL(12);                    \
+    case 24: return CALL(24);                    \
+    case 48: return CALL(48);                    \
+    case 96: return CALL(96);                    \
+    case 192: return CALL(192);                  \
+    case 384: return CALL(384);                  \
+    case 768: return CALL(768);                  \
     default: return cudaErrorInvalidValue;       \
   }
 

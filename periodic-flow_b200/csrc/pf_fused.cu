@@ -509,9 +509,9 @@ void fused_destroy(FusedPlan* p) {
 template <int N, int E, int T> static cudaError_t p1_run(FusedPlan* p, const float2* uh,
                                                         cudaStream_t st) {
   constexpr int G = N / E;
-  const float2* tw = tw_base<float>() + (N - 2);
+  const float2* tw = tw_base<float>() + tw_offset(N);
   const long long ncols = (long long)p->f.c1 * p->f.c2;
-  const size_t sm = G > 1 ? sizeof(float2) * N * T : 0;
+  const size_t sm = Plan<N, E>::stages() > 1 ? sizeof(float2) * N * T : 0;
   cudaError_t e = set_smem(k_p1<float, N, E, T>, sm);
   if (e != cudaSuccess) return e;
   k_p1<float, N, E, T><<<(unsigned)((ncols + T - 1) / T), dim3(T, G), sm, st>>>(
@@ -521,9 +521,9 @@ template <int N, int E, int T> static cudaError_t p1_run(FusedPlan* p, const flo
 
 template <int N, int E, int T> static cudaError_t p2_run(FusedPlan* p, cudaStream_t st) {
   constexpr int G = N / E;
-  const float2* tw = tw_base<float>() + (N - 2);
+  const float2* tw = tw_base<float>() + tw_offset(N);
   const long long ncols = (long long)p->f.n0 * p->f.c2;
-  const size_t sm = G > 1 ? sizeof(float2) * N * T : 0;
+  const size_t sm = Plan<N, E>::stages() > 1 ? sizeof(float2) * N * T : 0;
   cudaError_t e = set_smem(k_p2<float, N, E, T>, sm);
   if (e != cudaSuccess) return e;
   k_p2<float, N, E, T><<<(unsigned)((ncols + T - 1) / T), dim3(T, G), sm, st>>>(
@@ -534,9 +534,9 @@ template <int N, int E, int T> static cudaError_t p2_run(FusedPlan* p, cudaStrea
 template <int N, int E, int T> static cudaError_t p4_run(FusedPlan* p, float2* nl,
                                                         cudaStream_t st) {
   constexpr int G = N / E;
-  const float2* tw = tw_base<float>() + (N - 2);
+  const float2* tw = tw_base<float>() + tw_offset(N);
   const long long ncols = (long long)3 * p->f.n0 * p->f.nh;
-  const size_t sm = G > 1 ? sizeof(float2) * N * T : 0;
+  const size_t sm = Plan<N, E>::stages() > 1 ? sizeof(float2) * N * T : 0;
   cudaError_t e = set_smem(k_p4<float, N, E, T>, sm);
   if (e != cudaSuccess) return e;
   k_p4<float, N, E, T><<<(unsigned)((ncols + T - 1) / T), dim3(T, G), sm, st>>>(nl, p->f, tw);
@@ -573,7 +573,7 @@ static cudaError_t p3_n(FusedPlan* p, float2* nl, unsigned long long* maxbits, c
     return cudaErrorInvalidValue;
   } else {
     using TN = TuneC<N>;
-    const float2* tw = tw_base<float>() + (N - 2);
+    const float2* tw = tw_base<float>() + tw_offset(N);
     const long long ngroups = (long long)p->f.n0 * p->f.n1 / (2 * TN::PW);
     const int fb = 2 * TN::PW * p->f.c2;
     const int WC = ((2 * 6 * fb + TN::PW * (N + (N >> 4) + 1)) + 15) & ~15;
@@ -593,7 +593,7 @@ template <int N>
 static cudaError_t p5_n(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, const float2* nl,
                         cudaStream_t st) {
   using TN = TuneU<N>;
-  const float2* tw = tw_base<float>() + (N - 2);
+  const float2* tw = tw_base<float>() + tw_offset(N);
   const long long ncols = (long long)p->f.n1 * p->f.nh;
   const size_t sm = sizeof(float2) * 3 * N * TN::T;
   const dim3 grid((unsigned)((ncols + TN::T - 1) / TN::T)), block(TN::T, TN::G);

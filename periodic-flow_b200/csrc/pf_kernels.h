@@ -65,6 +65,13 @@ cudaError_t launch_curl_masked(cx<R>* dst, const cx<R>* u, const Geo& g, cudaStr
 template <typename R>
 cudaError_t launch_cross(R* u, const R* w, const Geo& g, unsigned long long* maxbits, cudaStream_t st);
 cudaError_t launch_set_dt(double* dscal, const unsigned long long* maxbits, double cfl, cudaStream_t st);
+// 3/2 rule: N-grid spectrum (or its curl) onto the M = 3N/2 grid, and back
+template <typename R>
+cudaError_t launch_pad(cx<R>* dst, const cx<R>* src, const Geo& gN, const Geo& gM, int ncomp,
+                       int curl, cudaStream_t st);
+template <typename R>
+cudaError_t launch_truncate(cx<R>* dst, const cx<R>* src, const Geo& gN, const Geo& gM,
+                            int ncomp, cudaStream_t st);
 cudaError_t launch_advance_time(double* dscal, int n, cudaStream_t st);
 template <typename R>
 cudaError_t launch_band_energy(const cx<R>* u, const Geo& g, double kf2, double* dscal,

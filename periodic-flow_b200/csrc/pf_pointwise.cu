@@ -261,6 +261,130 @@ __global__ void k_spectrum(const cx<R>* __restrict__ u, Geo g, double* out, int 
   }
 }
 
+// ------------------------------------------------- 3/2 padding / truncation
+// Grid M = 3N/2 per axis.  Padding writes the trigonometric polynomial of an
+// N-grid spectrum onto the M grid: a Nyquist mode of an even side is split in
+// half between +N/2 and -N/2 (complex axes) or halved (last axis, whose -N/2
+// partner is implied by Hermitian symmetry).  Truncation is the matching fold:
+// modes |k| < N/2 are copied, Nyquist modes sum their +N/2 and -N/2 partners.
+struct AxisMap { int j[2]; int n; };
+
+PF_D AxisMap pad_targets(int i, int N, int M) {
+  AxisMap a;
+  if ((N % 2 == 0) && i == N / 2) {
+    a.n = 2; a.j[0] = N / 2; a.j[1] = M - N / 2;
+  } else {
+    const int k = kfreq(i, N);
+    a.n = 1; a.j[0] = k >= 0 ? k : M + k; a.j[1] = 0;
+  }
+  return a;
+}
+
+template <typename R, int D>
+__global__ void k_pad(cx<R>* __restrict__ dst, const cx<R>* __restrict__ src, Geo gN, Geo gM,
+                      int ncomp, int curl) {
+  using C = cx<R>;
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < gN.nspec;
+       m += (long long)gridDim.x * blockDim.x) {
+    const ModeK<R, D> q = mode_k<R, D>(gN, m);
+    C val[3];
+    int nout = ncomp;
+    if (curl) {
+      // i k x u on the N grid (math.py:31-49), then padded
+      if constexpr (D == 2) {
+        const C a0 = src[m], a1 = src[gN.nspec + m];
+        val[0] = cmuli(csub(cscale(a1, q.k[0]), cscale(a0, q.k[1])));
+        nout = 1;
+      } else {
+        const C a0 = src[m], a1 = src[gN.nspec + m], a2 = src[2 * gN.nspec + m];
+        val[0] = cmuli(csub(cscale(a2, q.k[1]), cscale(a1, q.k[2])));
+        val[1] = cmuli(csub(cscale(a0, q.k[2]), cscale(a2, q.k[0])));
+        val[2] = cmuli(csub(cscale(a1, q.k[0]), cscale(a0, q.k[1])));
+        nout = 3;
+      }
+    } else {
+      for (int c = 0; c < ncomp; ++c) val[c] = src[c * gN.nspec + m];
+    }
+    const int il = D == 3 ? q.ix.i2 : q.ix.i1;
+    const int nl = gN.n[D - 1];
+    const R fl = ((nl % 2 == 0) && il == nl / 2) ? R(0.5) : R(1);
+    const AxisMap a0 = pad_targets(q.ix.i0, gN.n[0], gM.n[0]);
+    AxisMap a1;
+    if constexpr (D == 3) a1 = pad_targets(q.ix.i1, gN.n[1], gM.n[1]);
+    else { a1.n = 1; a1.j[0] = 0; }
+    const R f0 = a0.n == 2 ? R(0.5) : R(1), f1 = a1.n == 2 ? R(0.5) : R(1);
+    for (int s0 = 0; s0 < a0.n; ++s0)
+      for (int s1 = 0; s1 < a1.n; ++s1) {
+        const long long dm = D == 3 ? ((long long)a0.j[s0] * gM.s[1] + a1.j[s1]) * gM.nh + il
+                                    : (long long)a0.j[s0] * gM.nh + il;
+        for (int c = 0; c < nout; ++c) dst[c * gM.nspec + dm] = cscale(val[c], f0 * f1 * fl);
+      }
+  }
+}
+
+template <typename R, int D>
+__global__ void k_truncate(cx<R>* __restrict__ dst, const cx<R>* __restrict__ src, Geo gN,
+                           Geo gM, int ncomp) {
+  using C = cx<R>;
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < gN.nspec;
+       m += (long long)gridDim.x * blockDim.x) {
+    const ModeIdx ix = mode_index(gN, m);
+    const int il = D == 3 ? ix.i2 : ix.i1;
+    const int nl = gN.n[D - 1];
+    const bool nyq_last = (nl % 2 == 0) && il == nl / 2;
+    const AxisMap a0 = pad_targets(ix.i0, gN.n[0], gM.n[0]);
+    AxisMap a1;
+    if constexpr (D == 3) a1 = pad_targets(ix.i1, gN.n[1], gM.n[1]);
+    else { a1.n = 1; a1.j[0] = 0; }
+    for (int c = 0; c < ncomp; ++c) {
+      C acc = czero<C>();
+      for (int s0 = 0; s0 < a0.n; ++s0)
+        for (int s1 = 0; s1 < a1.n; ++s1) {
+          const int j0 = a0.j[s0], j1 = a1.j[s1];
+          const long long sm = D == 3 ? ((long long)j0 * gM.s[1] + j1) * gM.nh + il
+                                      : (long long)j0 * gM.nh + il;
+          acc = cadd(acc, src[c * gM.nspec + sm]);
+          if (nyq_last) {  // the -N/2 partner: conjugate of the mirror mode
+            const int r0 = (gM.n[0] - j0) % gM.n[0];
+            const int r1 = D == 3 ? (gM.n[1] - j1) % gM.n[1] : 0;
+            const long long mm = D == 3 ? ((long long)r0 * gM.s[1] + r1) * gM.nh + il
+                                        : (long long)r0 * gM.nh + il;
+            acc = cadd(acc, cconj(src[c * gM.nspec + mm]));
+          }
+        }
+      dst[c * gN.nspec + m] = acc;
+    }
+  }
+}
+
+template <typename R>
+cudaError_t launch_pad(cx<R>* dst, const cx<R>* src, const Geo& gN, const Geo& gM, int ncomp,
+                       int curl, cudaStream_t st) {
+  const int nout = curl ? (gN.dim == 3 ? 3 : 1) : ncomp;
+  cudaError_t e = cudaMemsetAsync(dst, 0, sizeof(cx<R>) * (size_t)nout * gM.nspec, st);
+  if (e != cudaSuccess) return e;
+  if (gN.dim == 3) k_pad<R, 3><<<grid_for(gN.nspec), kBlock, 0, st>>>(dst, src, gN, gM, ncomp, curl);
+  else k_pad<R, 2><<<grid_for(gN.nspec), kBlock, 0, st>>>(dst, src, gN, gM, ncomp, curl);
+  return launched();
+}
+
+template <typename R>
+cudaError_t launch_truncate(cx<R>* dst, const cx<R>* src, const Geo& gN, const Geo& gM,
+                            int ncomp, cudaStream_t st) {
+  if (gN.dim == 3) k_truncate<R, 3><<<grid_for(gN.nspec), kBlock, 0, st>>>(dst, src, gN, gM, ncomp);
+  else k_truncate<R, 2><<<grid_for(gN.nspec), kBlock, 0, st>>>(dst, src, gN, gM, ncomp);
+  return launched();
+}
+
+template cudaError_t launch_pad<float>(float2*, const float2*, const Geo&, const Geo&, int, int,
+                                       cudaStream_t);
+template cudaError_t launch_pad<double>(double2*, const double2*, const Geo&, const Geo&, int,
+                                        int, cudaStream_t);
+template cudaError_t launch_truncate<float>(float2*, const float2*, const Geo&, const Geo&, int,
+                                            cudaStream_t);
+template cudaError_t launch_truncate<double>(double2*, const double2*, const Geo&, const Geo&,
+                                             int, cudaStream_t);
+
 // -------------------------------------------------------------- launchers
 template <typename R>
 cudaError_t launch_update(const UpdateArgs<R>& A, int ncomp, cudaStream_t st) {

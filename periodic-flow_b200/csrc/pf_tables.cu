@@ -54,14 +54,17 @@ cudaError_t ensure_tables() {
   if ((int)done.size() > dev && done[dev]) return cudaSuccess;
   std::vector<float2> f(kTwSize);
   std::vector<double2> d(kTwSize);
-  for (int n = 2; n <= kMaxFFT; n *= 2) {
+  auto fill = [&](int n) {
+    const int off = tw_offset(n);
     for (int m = 0; m < n; ++m) {
       double c, s;
       root_of_unity(m, n, &c, &s);
-      d[n - 2 + m] = make_double2(c, s);
-      f[n - 2 + m] = make_float2((float)c, (float)s);
+      d[off + m] = make_double2(c, s);
+      f[off + m] = make_float2((float)c, (float)s);
     }
-  }
+  };
+  for (int n = 2; n <= kMaxFFT; n *= 2) fill(n);
+  for (int n = 12; n <= kMax3FFT; n *= 2) fill(n);
   e = cudaMemcpyToSymbol(g_tw_f32, f.data(), sizeof(float2) * kTwSize);
   if (e != cudaSuccess) return e;
   e = cudaMemcpyToSymbol(g_tw_f64, d.data(), sizeof(double2) * kTwSize);

@@ -19,7 +19,8 @@ NOISE_SOURCES = ("philox", "numpy", "injected")
 
 
 def build_config(Ns, domain, is_nonlinear, integrator_id, viscosity, noise_type, noise_mag,
-                 mask_nyquist, precision, dt, seed, noise_source, forcing, cfl, fused):
+                 mask_nyquist, precision, dt, seed, noise_source, forcing, cfl, fused,
+                 dealias="truncate"):
     """The pf_config of a solver (include/periodicflow_b200.h)."""
     dim = len(Ns)
     cfg = N.PfConfig()
@@ -35,7 +36,7 @@ def build_config(Ns, domain, is_nonlinear, integrator_id, viscosity, noise_type,
     cfg.viscosity = viscosity
     cfg.noise_type = N.PF_NOISE_THERMAL if noise_type == "thermal" else N.PF_NOISE_CORRELATED
     cfg.noise_mag = noise_mag
-    cfg.dealias = N.PF_DEALIAS_TRUNCATE
+    cfg.dealias = N.PF_DEALIAS_PAD if dealias == "pad" else N.PF_DEALIAS_TRUNCATE
     cfg.mask_nyquist = int(bool(mask_nyquist))
     cfg.precision = N.PF_FP64 if precision == "fp64" else N.PF_FP32
     cfg.dt = dt
@@ -70,9 +71,6 @@ class SpaceSolver(FourierSpace):
             raise ValueError(f"noise_source must be one of {NOISE_SOURCES}")
         if precision not in ("fp32", "fp64"):
             raise ValueError("precision must be 'fp32' or 'fp64'")
-        if is_nonlinear and self.dealias_rule == "pad":
-            raise NotImplementedError(
-                "dealias='3/2' (padding) is not built for the nonlinear term; use dealias='2/3'")
         self._is_nonlinear = is_nonlinear
         self.viscosity = viscosity
         self.noise_type = noise_type
@@ -91,7 +89,7 @@ class SpaceSolver(FourierSpace):
         self.forcing_cfg = forcing
         cfg = build_config(self.N, self.domain, is_nonlinear, integrator_id, viscosity,
                            noise_type, noise_mag, self.nyquist_mask is not None, precision, dt,
-                           seed, noise_source, forcing, cfl, fused)
+                           seed, noise_source, forcing, cfl, fused, dealias=self.dealias_rule)
         h = C.c_void_p()
         N.check(N.lib().pf_create(C.byref(cfg), C.byref(h)), None, "pf_create")
         self._h = h

@@ -90,5 +90,10 @@ def test_invalid_config_rejected_before_device_use():
     assert rc == N.PF_OK + 1
     assert b"2D and 3D" in N.lib().pf_last_error(None)
     cfg.dim = 3
-    cfg.n[1] = 48
+    cfg.n[1] = 40  # 5 * 8: only 2^b and 3 * 2^b lengths are built
     assert N.lib().pf_create(ctypes.byref(cfg), ctypes.byref(h)) == 3
+    cfg.n[1] = 48
+    cfg.dealias = N.PF_DEALIAS_PAD  # padded side 72 = 9 * 8 is not built
+    assert N.lib().pf_create(ctypes.byref(cfg), ctypes.byref(h)) == 3
+    cfg.dealias = 7
+    assert N.lib().pf_create(ctypes.byref(cfg), ctypes.byref(h)) == 1
