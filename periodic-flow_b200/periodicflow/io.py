@@ -1,13 +1,17 @@
 """Snapshot writer with the reference's interface (io.py:15-196).
 
-Snapshots of the physical velocity are taken from the device at write time.
-``reconfigure_dataset`` produces the reference's flat layout
-{x, y[, z], t, <var>/<zero-padded step>} with the optional periodic point;
-it is written as HDF5 when h5py is importable, else as ``<file>.npz`` with the
-same keys.
+``write(step)`` takes the physical velocity off the device and streams it to
+``<file>.snapshots/<step>.npy`` (memory stays flat however many snapshots a
+run writes).  ``reconfigure_dataset`` produces the reference's flat layout
+{x, y[, z], t, <var>/<zero-padded step>} with the optional periodic point
+(io.py:97-196): HDF5 when h5py is importable, else ``<file>.npz`` with the
+same keys, written member by member.
 """
 from __future__ import annotations
 
+import os
+import shutil
+import zipfile
 from pathlib import Path
 
 import numpy as np
@@ -28,18 +32,21 @@ class HDF5Writer:
         self.time_points = list(time_points)
         self.end_points = list(end_points)
         self.periodic = periodic
-        self.snapshots = {}  # step -> (d, N...) float64
+        self.snapdir = Path(self.file_name + ".snapshots")
+        if self.snapdir.exists():
+            shutil.rmtree(self.snapdir)
+        self.snapdir.mkdir(parents=True)
+        self.steps = []
         self.closed = False
 
     def write(self, step: int):
-        self.snapshots[int(step)] = self.solver.u
+        np.save(self.snapdir / f"{int(step)}.npy", self.solver.u)
+        self.steps.append(int(step))
 
     def close(self):
         self.closed = True
 
-    def _layout(self):
-        steps = sorted(self.snapshots)
-        nd = len(str(steps[-1])) if steps else 1
+    def _coords(self):
         out = {}
         for ax, (label, x_end) in enumerate(zip(["x", "y", "z"], self.end_points)):
             if ax >= self.solver.dim:
@@ -48,19 +55,24 @@ class HDF5Writer:
             if self.periodic:
                 coord = np.append(coord, x_end)
             out[label] = coord
-        out["t"] = np.linspace(self.time_points[0], self.time_points[-1], len(steps))
-        for s in steps:
-            for i, name in enumerate(self.names):
-                data = self.snapshots[s][i]
-                if self.periodic:
-                    data = periodic_bc(data)
-                out[f"{name}/{str(s).zfill(nd)}"] = data
+        out["t"] = np.linspace(self.time_points[0], self.time_points[-1], len(self.steps))
         return out
+
+    def _fields(self):
+        """Yield (key, array) one snapshot component at a time."""
+        steps = sorted(set(self.steps))
+        nd = len(str(steps[-1])) if steps else 1
+        for s in steps:
+            data = np.load(self.snapdir / f"{s}.npy")
+            for i, name in enumerate(self.names):
+                arr = data[i]
+                if self.periodic:
+                    arr = periodic_bc(arr)
+                yield f"{name}/{str(s).zfill(nd)}", arr
 
     def reconfigure_dataset(self):
         if self.mpi_rank == 0:
             logger.info("HDF5Writer.reconfigure_dataset: Start reconfiguring dataset.")
-        data = self._layout()
         path = Path(self.file_name).with_suffix(".h5")
         try:
             import h5py
@@ -68,11 +80,21 @@ class HDF5Writer:
             h5py = None
         if h5py is not None:
             with h5py.File(path, "w") as f:
-                for k, v in data.items():
+                for k, v in self._coords().items():
+                    f.create_dataset(k, data=v)
+                for k, v in self._fields():
                     f.create_dataset(k, data=v)
         else:
             path = path.with_suffix(".npz")
-            np.savez(path, **data)
+            with zipfile.ZipFile(path, "w", allowZip64=True) as zf:
+                items = list(self._coords().items())
+                for k, v in items:
+                    with zf.open(k + ".npy", "w", force_zip64=True) as fh:
+                        np.lib.format.write_array(fh, np.asarray(v))
+                for k, v in self._fields():
+                    with zf.open(k + ".npy", "w", force_zip64=True) as fh:
+                        np.lib.format.write_array(fh, np.asarray(v))
+        shutil.rmtree(self.snapdir, ignore_errors=True)
         if self.mpi_rank == 0:
             logger.info(f"HDF5Writer.reconfigure_dataset: Dataset written to {path}.")
         return path
