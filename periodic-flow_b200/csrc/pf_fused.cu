@@ -42,7 +42,22 @@ template <int N> struct TuneC {  // contiguous pass P3: 8 values per lane
   static constexpr int G = N / E;   // lanes per line pair, <= 32 for N <= 256
   static constexpr int PW = 32 / G; // line pairs per warp
   static constexpr int W = 8;       // warps per CTA
+  // exchange buffer of one line pair (8-byte values): position p lives at
+  // p ^ ((p >> 3) & 15), which spreads the radix-8 stage stores (stride 8)
+  // over all banks; the pair stride shifts neighbouring pairs' banks.  The
+  // sides up to 16 use a plain +1 per 16 padding instead.
+  static constexpr int BUF = N <= 16 ? N + 2 : (N == 32 ? N + 4 : (N == 64 ? N + 8 : N));
+  static PF_HD int sw(int p) { return N <= 16 ? p + (p >> 4) : p ^ ((p >> 3) & 15); }
 };
+
+// Exchange buffer of the strided passes: position p of column t.  Eight
+// padding values after every 16 positions put the radix-16 stage stores of
+// neighbouring threadIdx.y rows (positions 16 apart) on different banks when
+// T = 8.
+template <int T> PF_HD int col_pos(int p, int t) { return p * T + t + 8 * (p >> 4); }
+template <int N, int T> constexpr size_t col_buf_bytes() {
+  return sizeof(float2) * (size_t)(N * T + 8 * (N >> 4));
+}
 
 struct FGeo {
   int n0, n1, n2, nh;
@@ -61,12 +76,15 @@ struct FusedPlan {
   void* B = nullptr;  // 6 * n0 * n1 * c2 complex
   int* err = nullptr; // device error word (bounded waits that gave up)
   int nsm = 148;
-  int var[6] = {0, 0, 0, 0, 0, 0};  // launch variant per pass
+  // launch variant per pass (used where that pass's axis has 256 points):
+  // measured best on B200 at 256^3 are P1 (16, 8) at >= 4 CTAs per SM, P2
+  // (16, 8) at >= 3 CTAs per SM, P3 one staging buffer, 4 warps x 3 CTAs
+  int var[6] = {0, 5, 4, 2, 0, 0};
 };
 
 // ---------------------------------------------------------------------- P1
-template <typename R, int N, int E, int T>
-__global__ void __launch_bounds__(T * (N / E))
+template <typename R, int N, int E, int T, int MB>
+__global__ void __launch_bounds__(T * (N / E), MB)
 k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
      const cx<R>* __restrict__ tw) {
   constexpr int G = N / E;
@@ -88,7 +106,7 @@ k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
   const int row_in = f.n1 * f.nh;
   const int fs_out = N * ncols;
   const int fs_in = (int)f.nspec;
-  auto smf = [&](int pos) -> C& { return sm[pos * T + t]; };
+  auto smf = [&](int pos) -> C& { return sm[col_pos<T>(pos, t)]; };
   auto sync = [] { __syncthreads(); };
   // row e of the column: kept when |k0| <= kmax0 (recomputed, not stored)
   auto kept = [&](int e) { return active && abs(kfreq(j + G * e, N)) <= f.kmax0; };
@@ -120,8 +138,8 @@ k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
 }
 
 // ---------------------------------------------------------------------- P2
-template <typename R, int N, int E, int T>
-__global__ void __launch_bounds__(T * (N / E))
+template <typename R, int N, int E, int T, int MB>
+__global__ void __launch_bounds__(T * (N / E), MB)
 k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
      const cx<R>* __restrict__ tw) {
   constexpr int G = N / E;
@@ -143,7 +161,7 @@ k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
   }
   const int fs_in = f.n0 * f.c1 * f.c2;
   const int fs_out = f.n0 * N * f.c2;
-  auto smf = [&](int pos) -> C& { return sm[pos * T + t]; };
+  auto smf = [&](int pos) -> C& { return sm[col_pos<T>(pos, t)]; };
   auto sync = [] { __syncthreads(); };
   // per element e of the line (recomputed, not stored): kept flag, k1,
   // offset of the compact input index
@@ -200,36 +218,38 @@ k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
 // G lanes).  A group's six input fields are two adjacent lines each, so one
 // bulk copy per field lands a group in shared memory; the copy of the next
 // group (other stage) is in flight while the current one is transformed.
-template <typename R, int N>
-__global__ void __launch_bounds__(256, 1)
+template <typename R, int N, int NB, int W, int MB>
+__global__ void __launch_bounds__(32 * W, MB)
 k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
      const cx<R>* __restrict__ tw, unsigned long long* __restrict__ maxbits, R scale,
      int* __restrict__ err, long long ngroups) {
-  constexpr int E = TuneC<N>::E, G = TuneC<N>::G, PW = TuneC<N>::PW, W = TuneC<N>::W;
+  constexpr int E = TuneC<N>::E, G = TuneC<N>::G, PW = TuneC<N>::PW;
   constexpr int H = N / 2;
-  constexpr int SH = sizeof(R) == 4 ? 4 : 3;
-  constexpr int BUF = N + (N >> SH) + 1;
+  constexpr int BUF = TuneC<N>::BUF;
   static_assert(G <= 32 && 32 % G == 0, "line pairs tile a warp");
+  static_assert(NB == 1 || NB == 2, "one or two staging buffers per warp");
+  static_assert(NB * W <= 16, "mbarriers fit the 128-byte header");
   using C = cx<R>;
   extern __shared__ __align__(128) unsigned char smraw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int pw = lane / G, j = lane % G;
   const int fb = 2 * PW * f.c2;        // complex values of one field of a group
-  const int SC = 6 * fb;               // one stage
-  const int WC = ((2 * SC + PW * BUF) + 15) & ~15;
+  const int SC = 6 * fb;               // one staging buffer
+  const int WC = ((NB * SC + PW * BUF) + 15) & ~15;
   const uint32_t fbytes = (uint32_t)(fb * sizeof(C));
   const long long fs_in = (long long)f.n0 * f.n1 * f.c2;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smraw) + 2 * warp;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smraw) + NB * warp;
   C* wbase = reinterpret_cast<C*>(smraw + 128) + (long long)warp * WC;
-  C* ex = wbase + 2 * SC + pw * BUF;
+  C* ex = wbase + NB * SC + pw * BUF;
   if (lane == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
+#pragma unroll
+    for (int s = 0; s < NB; ++s) mbar_init(&bars[s], 1);
     fence_mbar_init();
   }
   __syncwarp();
   auto issue = [&](long long grp, int s) {
     if (lane == 0) {
+      fence_proxy_async_smem();
       mbar_arrive_expect_tx(&bars[s], 6 * fbytes);
       const C* src = B + grp * fb;
       C* dst = wbase + s * SC;
@@ -237,46 +257,61 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
       for (int fld = 0; fld < 6; ++fld) bulk_g2s(dst + fld * fb, src + fld * fs_in, fbytes, &bars[s]);
     }
   };
-  auto smf = [&](int pos) -> C& { return ex[pos + (pos >> SH)]; };
+  auto smf = [&](int pos) -> C& { return ex[TuneC<N>::sw(pos)]; };
   auto sync = [] { __syncwarp(); };
+  // line pair of one field: two adjacent half-spectrum lines a, b packed as
+  // z = a + i b on the full length-N circle (DC imaginary parts dropped)
+  auto unpack = [&](const C* pa, C (&z)[E]) {
+    const C* pb = pa + f.c2;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int m = j + G * e;
+      const int k = m <= H ? m : N - m;
+      const bool kin = k < f.c2;
+      C a = kin ? pa[k] : czero<C>();
+      C b = kin ? pb[k] : czero<C>();
+      if (m == 0) { a.y = 0; b.y = 0; }
+      C r;
+      if (m <= H) { r.x = a.x - b.y; r.y = a.y + b.x; }
+      else { r.x = a.x + b.y; r.y = b.x - a.y; }
+      z[e] = r;
+    }
+  };
   const long long TW = (long long)gridDim.x * W;
   long long g = (long long)blockIdx.x * W + warp;
   if (g < ngroups) issue(g, 0);
   double mx = 0.0;
   const R h = R(0.5) * scale;
   for (int it = 0; g < ngroups; g += TW, ++it) {
-    const int s = it & 1;
+    const int s = NB == 2 ? (it & 1) : 0;
     const bool more = g + TW < ngroups;
-    if (more) {
+    if (NB == 2 && more) {
       __syncwarp();
       issue(g + TW, s ^ 1);
     }
-    const bool ok = mbar_wait_bounded(&bars[s], (uint32_t)((it >> 1) & 1));
+    const uint32_t par = NB == 2 ? (uint32_t)((it >> 1) & 1) : (uint32_t)(it & 1);
+    const bool ok = mbar_wait_bounded(&bars[s], par);
     if (!__all_sync(0xffffffffu, ok)) {
       if (lane == 0) atomicExch(err, kErrWaitP3);
-      if (more) mbar_wait_bounded(&bars[s ^ 1], (uint32_t)(((it + 1) >> 1) & 1));
+      if (NB == 2 && more) mbar_wait_bounded(&bars[s ^ 1], (uint32_t)(((it + 1) >> 1) & 1));
       return;
     }
     const C* in = wbase + s * SC + 2 * pw * f.c2;
     C z[6][E];
+    if constexpr (NB == 1) {
+      // all six fields into registers, then the buffer takes the next group
 #pragma unroll
-    for (int fld = 0; fld < 6; ++fld) {
-      const C* pa = in + fld * fb;
-      const C* pb = pa + f.c2;
+      for (int fld = 0; fld < 6; ++fld) unpack(in + fld * fb, z[fld]);
+      __syncwarp();
+      if (more) issue(g + TW, 0);
 #pragma unroll
-      for (int e = 0; e < E; ++e) {
-        const int m = j + G * e;
-        const int k = m <= H ? m : N - m;
-        const bool kin = k < f.c2;
-        C a = kin ? pa[k] : czero<C>();
-        C b = kin ? pb[k] : czero<C>();
-        if (m == 0) { a.y = 0; b.y = 0; }
-        C r;
-        if (m <= H) { r.x = a.x - b.y; r.y = a.y + b.x; }
-        else { r.x = a.x + b.y; r.y = b.x - a.y; }
-        z[fld][e] = r;
+      for (int fld = 0; fld < 6; ++fld) fft<N, E, +1>(z[fld], j, tw, smf, sync);
+    } else {
+#pragma unroll
+      for (int fld = 0; fld < 6; ++fld) {
+        unpack(in + fld * fb, z[fld]);
+        fft<N, E, +1>(z[fld], j, tw, smf, sync);
       }
-      fft<N, E, +1>(z[fld], j, tw, smf, sync);
     }
     // u x omega for both lines (real parts: line a, imaginary parts: line b)
     C c[3][E];
@@ -330,8 +365,8 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
 // ---------------------------------------------------------------------- P4
 // In-place forward FFT along axis 1 of nl[3][x0][x1][k2]: column q = (plane,
 // k2) with plane = comp * n0 + x0.
-template <typename R, int N, int E, int T>
-__global__ void __launch_bounds__(T * (N / E))
+template <typename R, int N, int E, int T, int MB>
+__global__ void __launch_bounds__(T * (N / E), MB)
 k_p4(cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
   constexpr int G = N / E;
   using C = cx<R>;
@@ -350,7 +385,7 @@ k_p4(cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
 #pragma unroll
   for (int e = 0; e < E; ++e)
     v[e] = active ? nl[base + (long long)(j + G * e) * f.nh] : czero<C>();
-  fft<N, E, -1>(v, j, tw, [&](int pos) -> C& { return sm[pos * T + t]; },
+  fft<N, E, -1>(v, j, tw, [&](int pos) -> C& { return sm[col_pos<T>(pos, t)]; },
                 [] { __syncthreads(); });
   if (active) {
 #pragma unroll
@@ -503,43 +538,44 @@ void fused_destroy(FusedPlan* p) {
     default: return cudaErrorInvalidValue; \
   }
 
-// Launch variants (radix width E, columns per CTA T) of the strided passes;
-// variant 0 is the default of TuneS, 1..3 exist for n = 256 (tuning knob
-// PF_FUSED_VARIANT="p1:v,p2:v,p4:v").
-template <int N, int E, int T> static cudaError_t p1_run(FusedPlan* p, const float2* uh,
+// Launch variants (radix width E, columns per CTA T, minimum CTAs per SM MB
+// that caps registers; 0: no cap) of the strided passes; variant 0 is the
+// TuneS default, 1..6 exist for n = 256 (tuning knob
+// PF_FUSED_VARIANT="p1:v,p2:v,p3:v,p4:v", which overrides FusedPlan::var).
+template <int N, int E, int T, int MB = 0> static cudaError_t p1_run(FusedPlan* p, const float2* uh,
                                                         cudaStream_t st) {
   constexpr int G = N / E;
   const float2* tw = tw_base<float>() + tw_offset(N);
   const long long ncols = (long long)p->f.c1 * p->f.c2;
-  const size_t sm = Plan<N, E>::stages() > 1 ? sizeof(float2) * N * T : 0;
-  cudaError_t e = set_smem(k_p1<float, N, E, T>, sm);
+  const size_t sm = Plan<N, E>::stages() > 1 ? col_buf_bytes<N, T>() : 0;
+  cudaError_t e = set_smem(k_p1<float, N, E, T, MB>, sm);
   if (e != cudaSuccess) return e;
-  k_p1<float, N, E, T><<<(unsigned)((ncols + T - 1) / T), dim3(T, G), sm, st>>>(
+  k_p1<float, N, E, T, MB><<<(unsigned)((ncols + T - 1) / T), dim3(T, G), sm, st>>>(
       uh, (float2*)p->A, p->f, tw);
   return launched();
 }
 
-template <int N, int E, int T> static cudaError_t p2_run(FusedPlan* p, cudaStream_t st) {
+template <int N, int E, int T, int MB = 0> static cudaError_t p2_run(FusedPlan* p, cudaStream_t st) {
   constexpr int G = N / E;
   const float2* tw = tw_base<float>() + tw_offset(N);
   const long long ncols = (long long)p->f.n0 * p->f.c2;
-  const size_t sm = Plan<N, E>::stages() > 1 ? sizeof(float2) * N * T : 0;
-  cudaError_t e = set_smem(k_p2<float, N, E, T>, sm);
+  const size_t sm = Plan<N, E>::stages() > 1 ? col_buf_bytes<N, T>() : 0;
+  cudaError_t e = set_smem(k_p2<float, N, E, T, MB>, sm);
   if (e != cudaSuccess) return e;
-  k_p2<float, N, E, T><<<(unsigned)((ncols + T - 1) / T), dim3(T, G), sm, st>>>(
+  k_p2<float, N, E, T, MB><<<(unsigned)((ncols + T - 1) / T), dim3(T, G), sm, st>>>(
       (const float2*)p->A, (float2*)p->B, p->f, tw);
   return launched();
 }
 
-template <int N, int E, int T> static cudaError_t p4_run(FusedPlan* p, float2* nl,
+template <int N, int E, int T, int MB = 0> static cudaError_t p4_run(FusedPlan* p, float2* nl,
                                                         cudaStream_t st) {
   constexpr int G = N / E;
   const float2* tw = tw_base<float>() + tw_offset(N);
   const long long ncols = (long long)3 * p->f.n0 * p->f.nh;
-  const size_t sm = Plan<N, E>::stages() > 1 ? sizeof(float2) * N * T : 0;
-  cudaError_t e = set_smem(k_p4<float, N, E, T>, sm);
+  const size_t sm = Plan<N, E>::stages() > 1 ? col_buf_bytes<N, T>() : 0;
+  cudaError_t e = set_smem(k_p4<float, N, E, T, MB>, sm);
   if (e != cudaSuccess) return e;
-  k_p4<float, N, E, T><<<(unsigned)((ncols + T - 1) / T), dim3(T, G), sm, st>>>(nl, p->f, tw);
+  k_p4<float, N, E, T, MB><<<(unsigned)((ncols + T - 1) / T), dim3(T, G), sm, st>>>(nl, p->f, tw);
   return launched();
 }
 
@@ -549,6 +585,9 @@ template <int N, int E, int T> static cudaError_t p4_run(FusedPlan* p, float2* n
       case 1: return RUN<256, 8, 16>(__VA_ARGS__);                      \
       case 2: return RUN<256, 8, 32>(__VA_ARGS__);                      \
       case 3: return RUN<256, 16, 8>(__VA_ARGS__);                      \
+      case 4: return RUN<256, 16, 8, 3>(__VA_ARGS__);                   \
+      case 5: return RUN<256, 16, 8, 4>(__VA_ARGS__);                   \
+      case 6: return RUN<256, 16, 16, 2>(__VA_ARGS__);                  \
       default: break;                                                   \
     }                                                                   \
   }                                                                     \
@@ -567,25 +606,41 @@ template <int N> static cudaError_t p4_n(FusedPlan* p, float2* nl, cudaStream_t 
   PF_VARIANTS(p4_run, N, p, nl, st)
 }
 
+template <int N, int NB, int W, int MB>
+static cudaError_t p3_run(FusedPlan* p, float2* nl, unsigned long long* maxbits, cudaStream_t st) {
+  using TN = TuneC<N>;
+  const float2* tw = tw_base<float>() + tw_offset(N);
+  const long long ngroups = (long long)p->f.n0 * p->f.n1 / (2 * TN::PW);
+  const int fb = 2 * TN::PW * p->f.c2;
+  const int WC = ((NB * 6 * fb + TN::PW * TN::BUF) + 15) & ~15;
+  const size_t sm = 128 + sizeof(float2) * (size_t)W * WC;
+  cudaError_t e = set_smem(k_p3<float, N, NB, W, MB>, sm);
+  if (e != cudaSuccess) return e;
+  const float scale = (float)(1.0 / ((double)p->f.n0 * p->f.n1 * p->f.n2));
+  long long blocks = (ngroups + W - 1) / W;
+  if (blocks > (long long)p->nsm * MB) blocks = (long long)p->nsm * MB;
+  k_p3<float, N, NB, W, MB><<<(unsigned)blocks, 32 * W, sm, st>>>(
+      (const float2*)p->B, nl, p->f, tw, maxbits, scale, p->err, ngroups);
+  return launched();
+}
+
+// Variant 0: two staging buffers per warp, 8 warps, one CTA per SM; 1..3
+// (n2 = 256): one staging buffer refilled as soon as the group is in
+// registers, with 8 warps x 2 CTAs, 4 warps x 3 CTAs or 8 warps x 1 CTA.
 template <int N>
 static cudaError_t p3_n(FusedPlan* p, float2* nl, unsigned long long* maxbits, cudaStream_t st) {
   if constexpr (N > 256) {
     return cudaErrorInvalidValue;
   } else {
-    using TN = TuneC<N>;
-    const float2* tw = tw_base<float>() + tw_offset(N);
-    const long long ngroups = (long long)p->f.n0 * p->f.n1 / (2 * TN::PW);
-    const int fb = 2 * TN::PW * p->f.c2;
-    const int WC = ((2 * 6 * fb + TN::PW * (N + (N >> 4) + 1)) + 15) & ~15;
-    const size_t sm = 128 + sizeof(float2) * (size_t)TN::W * WC;
-    cudaError_t e = set_smem(k_p3<float, N>, sm);
-    if (e != cudaSuccess) return e;
-    const float scale = (float)(1.0 / ((double)p->f.n0 * p->f.n1 * p->f.n2));
-    long long blocks = (ngroups + TN::W - 1) / TN::W;
-    if (blocks > p->nsm) blocks = p->nsm;
-    k_p3<float, N><<<(unsigned)blocks, 32 * TN::W, sm, st>>>(
-        (const float2*)p->B, nl, p->f, tw, maxbits, scale, p->err, ngroups);
-    return launched();
+    if constexpr (N == 256) {
+      switch (p->var[3]) {
+        case 1: return p3_run<256, 1, 8, 2>(p, nl, maxbits, st);
+        case 2: return p3_run<256, 1, 4, 3>(p, nl, maxbits, st);
+        case 3: return p3_run<256, 1, 8, 1>(p, nl, maxbits, st);
+        default: break;
+      }
+    }
+    return p3_run<N, 2, TuneC<N>::W, 1>(p, nl, maxbits, st);
   }
 }
 

@@ -26,6 +26,10 @@ PF_D void mbar_init(uint64_t* bar, uint32_t count) {
 // make mbarrier initialisation visible to the async proxy
 PF_D void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
+// order earlier generic-proxy accesses of shared memory before later
+// async-proxy (bulk copy) writes to it
+PF_D void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
 PF_D void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
                "r"(bytes)
