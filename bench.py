@@ -56,6 +56,12 @@ def pass_bytes(n):
     }
 
 
+# DRAM bytes (read + write) per launch at n = 256 from one ncu --set full
+# capture of k_p3 / k_p5 under "bench.py --steps 10 --warmup 3 --no-e2e
+# --no-cpu --no-ensemble".
+NCU_TRAFFIC_256 = {3: 270.600192e6 + 157.152512e6, 5: 608.803840e6 + 171.791104e6}
+
+
 def _dist():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     if ws > 1:
@@ -198,10 +204,14 @@ def run_ours(args, dist, rank, world):
     avg_s = tot_ms.value / max(nl.value, 1) / 1e3
     alg = pb[f"P{args.timed_pass}"]
     achieved = alg / avg_s / 1e9 if avg_s > 0 else None
+    traffic, traffic_src = args.traffic, "--traffic"
+    if traffic is None and n == 256 and args.timed_pass in NCU_TRAFFIC_256:
+        traffic, traffic_src = NCU_TRAFFIC_256[args.timed_pass], "ncu capture at 256^3"
     roofline = {"bound": "hbm", "kernel": f"fused pass P{args.timed_pass}",
                 "achieved": achieved, "peak": peak, "peak_source": peak_src, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None,
-                "traffic": args.traffic, "alg_bytes_per_launch": alg,
+                "traffic": traffic, "traffic_source": traffic_src if traffic else None,
+                "alg_bytes_per_launch": alg,
                 "avg_launch_ms": avg_s * 1e3, "launches_timed": nl.value}
     step_bytes = 3 * sum(pb[f"P{i}"] for i in range(1, 6))
     step_roof = {"alg_bytes_per_step": step_bytes,

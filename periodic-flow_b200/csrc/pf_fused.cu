@@ -398,11 +398,11 @@ k_p4(cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
 // N x T buffer per component, also the FFT's exchange buffer) so the update
 // phase holds only a chunk of modes in registers; u_hat / u0 of a chunk are
 // loaded before any of its stores.
-template <typename R, int N, int NC, bool NOISE>
+template <typename R, int N, int NC, bool NOISE, int CHU>
 __global__ void __launch_bounds__(TuneU<N>::T * TuneU<N>::G, 2)
 k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
   constexpr int E = TuneU<N>::E, G = TuneU<N>::G, T = TuneU<N>::T;
-  constexpr int CH = E < 4 ? E : 4;
+  constexpr int CH = E < CHU ? E : CHU;  // rows per thread whose state loads are in flight
   using C = cx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* S = reinterpret_cast<C*>(smraw);
@@ -644,9 +644,9 @@ static cudaError_t p3_n(FusedPlan* p, float2* nl, unsigned long long* maxbits, c
   }
 }
 
-template <int N>
-static cudaError_t p5_n(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, const float2* nl,
-                        cudaStream_t st) {
+template <int N, int CH>
+static cudaError_t p5_run(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, const float2* nl,
+                          cudaStream_t st) {
   using TN = TuneU<N>;
   const float2* tw = tw_base<float>() + tw_offset(N);
   const long long ncols = (long long)p->f.n1 * p->f.nh;
@@ -654,19 +654,34 @@ static cudaError_t p5_n(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, con
   const dim3 grid((unsigned)((ncols + TN::T - 1) / TN::T)), block(TN::T, TN::G);
   cudaError_t e;
   if (U.noise_src == kNoiseNone) {
-    e = set_smem(k_p5<float, N, 3, false>, sm);
+    e = set_smem(k_p5<float, N, 3, false, CH>, sm);
     if (e != cudaSuccess) return e;
-    k_p5<float, N, 3, false><<<grid, block, sm, st>>>(U, nl, p->f, tw);
+    k_p5<float, N, 3, false, CH><<<grid, block, sm, st>>>(U, nl, p->f, tw);
   } else if (ncomp == 9) {
-    e = set_smem(k_p5<float, N, 9, true>, sm);
+    e = set_smem(k_p5<float, N, 9, true, CH>, sm);
     if (e != cudaSuccess) return e;
-    k_p5<float, N, 9, true><<<grid, block, sm, st>>>(U, nl, p->f, tw);
+    k_p5<float, N, 9, true, CH><<<grid, block, sm, st>>>(U, nl, p->f, tw);
   } else {
-    e = set_smem(k_p5<float, N, 3, true>, sm);
+    e = set_smem(k_p5<float, N, 3, true, CH>, sm);
     if (e != cudaSuccess) return e;
-    k_p5<float, N, 3, true><<<grid, block, sm, st>>>(U, nl, p->f, tw);
+    k_p5<float, N, 3, true, CH><<<grid, block, sm, st>>>(U, nl, p->f, tw);
   }
   return launched();
+}
+
+// Variant 0 keeps the state loads of 4 rows per thread in flight; 1, 2
+// (n0 = 256) use 2 and 8.
+template <int N>
+static cudaError_t p5_n(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, const float2* nl,
+                        cudaStream_t st) {
+  if constexpr (N == 256) {
+    switch (p->var[5]) {
+      case 1: return p5_run<256, 2>(p, U, ncomp, nl, st);
+      case 2: return p5_run<256, 8>(p, U, ncomp, nl, st);
+      default: break;
+    }
+  }
+  return p5_run<N, 4>(p, U, ncomp, nl, st);
 }
 
 cudaError_t fused_pass(FusedPlan* p, int pass, const void* uhat, void* nl,
