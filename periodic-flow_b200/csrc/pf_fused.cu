@@ -77,9 +77,12 @@ struct FusedPlan {
   int* err = nullptr; // device error word (bounded waits that gave up)
   int nsm = 148;
   // launch variant per pass (used where that pass's axis has 256 points):
-  // measured best on B200 at 256^3 are P1 (16, 8) at >= 4 CTAs per SM, P2
-  // (16, 8) at >= 3 CTAs per SM, P3 one staging buffer, 4 warps x 3 CTAs
-  int var[6] = {0, 5, 4, 2, 0, 0};
+  // measured best on B200 at 256^3 are P1 and P2 (16, 8) at >= 4 CTAs per
+  // SM, P3 one staging buffer, 4 warps x 3 CTAs
+  int var[6] = {0, 5, 5, 2, 0, 0};
+  // CTA rows per column tile of P1 (1 or 3) and P2 (1 or 2): one per group
+  // of fields (PF_FUSED_SPLIT="p1:v,p2:v" overrides)
+  int split[6] = {1, 3, 2, 1, 1, 1};
 };
 
 // ---------------------------------------------------------------------- P1
@@ -110,16 +113,22 @@ k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
   auto sync = [] { __syncthreads(); };
   // row e of the column: kept when |k0| <= kmax0 (recomputed, not stored)
   auto kept = [&](int e) { return active && abs(kfreq(j + G * e, N)) <= f.kmax0; };
+  // gridDim.y == 3: block row y transforms field y alone (u0; u1 and D1;
+  // u2 and D2), which triples the CTAs without extra traffic
+  const int part = gridDim.y == 1 ? -1 : (int)blockIdx.y;
   C v[E], w[E];
+  if (part <= 0) {
 #pragma unroll
-  for (int e = 0; e < E; ++e) v[e] = kept(e) ? uh[(j + G * e) * row_in + in_off] : czero<C>();
-  fft<N, E, +1>(v, j, tw, smf, sync);
-  if (active) {
+    for (int e = 0; e < E; ++e) v[e] = kept(e) ? uh[(j + G * e) * row_in + in_off] : czero<C>();
+    fft<N, E, +1>(v, j, tw, smf, sync);
+    if (active) {
 #pragma unroll
-    for (int e = 0; e < E; ++e) A[(j + G * e) * ncols + q] = v[e];
+      for (int e = 0; e < E; ++e) A[(j + G * e) * ncols + q] = v[e];
+    }
   }
 #pragma unroll
   for (int c = 1; c <= 2; ++c) {
+    if (part >= 0 && part != c) continue;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       v[e] = kept(e) ? uh[c * fs_in + (j + G * e) * row_in + in_off] : czero<C>();
@@ -177,40 +186,47 @@ k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
       for (int e = 0; e < E; ++e) B[fld * fs_out + out_base + (j + G * e) * f.c2] = v[e];
     }
   };
+  // gridDim.y == 2: block row 0 makes omega0, u1, u2 (reads u1, u2), row 1
+  // omega2, omega1, u0 (reads u0, D1, D2); twice the CTAs, no extra traffic
+  const int part = gridDim.y == 1 ? -1 : (int)blockIdx.y;
   C a[E], b[E], w[E];
-  // omega0 = i (k1 u2 - k2 u1); u1; u2
+  if (part <= 0) {
+    // omega0 = i (k1 u2 - k2 u1); u1; u2
 #pragma unroll
-  for (int e = 0; e < E; ++e) {
-    const bool kp = kept(e);
-    a[e] = kp ? A[1 * fs_in + off(e)] : czero<C>();
-    b[e] = kp ? A[2 * fs_in + off(e)] : czero<C>();
-    w[e] = cmuli(csub(cscale(b[e], k1(e)), cscale(a[e], k2)));
+    for (int e = 0; e < E; ++e) {
+      const bool kp = kept(e);
+      a[e] = kp ? A[1 * fs_in + off(e)] : czero<C>();
+      b[e] = kp ? A[2 * fs_in + off(e)] : czero<C>();
+      w[e] = cmuli(csub(cscale(b[e], k1(e)), cscale(a[e], k2)));
+    }
+    fft<N, E, +1>(w, j, tw, smf, sync);
+    store(3, w);
+    fft<N, E, +1>(a, j, tw, smf, sync);
+    store(1, a);
+    fft<N, E, +1>(b, j, tw, smf, sync);
+    store(2, b);
   }
-  fft<N, E, +1>(w, j, tw, smf, sync);
-  store(3, w);
-  fft<N, E, +1>(a, j, tw, smf, sync);
-  store(1, a);
-  fft<N, E, +1>(b, j, tw, smf, sync);
-  store(2, b);
-  // omega2 = D1 - i k1 u0; omega1 = i k2 u0 - D2; u0
+  if (part != 0) {
+    // omega2 = D1 - i k1 u0; omega1 = i k2 u0 - D2; u0
 #pragma unroll
-  for (int e = 0; e < E; ++e) {
-    const bool kp = kept(e);
-    a[e] = kp ? A[0 * fs_in + off(e)] : czero<C>();
-    b[e] = kp ? A[3 * fs_in + off(e)] : czero<C>();
-    w[e] = csub(b[e], cmuli(cscale(a[e], k1(e))));
-  }
-  fft<N, E, +1>(w, j, tw, smf, sync);
-  store(5, w);
+    for (int e = 0; e < E; ++e) {
+      const bool kp = kept(e);
+      a[e] = kp ? A[0 * fs_in + off(e)] : czero<C>();
+      b[e] = kp ? A[3 * fs_in + off(e)] : czero<C>();
+      w[e] = csub(b[e], cmuli(cscale(a[e], k1(e))));
+    }
+    fft<N, E, +1>(w, j, tw, smf, sync);
+    store(5, w);
 #pragma unroll
-  for (int e = 0; e < E; ++e) {
-    b[e] = kept(e) ? A[4 * fs_in + off(e)] : czero<C>();
-    w[e] = csub(cmuli(cscale(a[e], k2)), b[e]);
+    for (int e = 0; e < E; ++e) {
+      b[e] = kept(e) ? A[4 * fs_in + off(e)] : czero<C>();
+      w[e] = csub(cmuli(cscale(a[e], k2)), b[e]);
+    }
+    fft<N, E, +1>(w, j, tw, smf, sync);
+    store(4, w);
+    fft<N, E, +1>(a, j, tw, smf, sync);
+    store(0, a);
   }
-  fft<N, E, +1>(w, j, tw, smf, sync);
-  store(4, w);
-  fft<N, E, +1>(a, j, tw, smf, sync);
-  store(0, a);
 }
 
 // ---------------------------------------------------------------------- P3
@@ -503,7 +519,14 @@ FusedPlan* fused_create(const Geo& g, int precision, int dealias) {
     // "p1:1,p2:2,p4:1"
     for (const char* c = v; *c; ++c)
       if (c[0] == 'p' && c[1] >= '1' && c[1] <= '5' && c[2] == ':') p->var[c[1] - '0'] = atoi(c + 3);
+  }  if (const char* v = getenv("PF_FUSED_SPLIT")) {
+    for (const char* c = v; *c; ++c)
+      if (c[0] == 'p' && (c[1] == '1' || c[1] == '2') && c[2] == ':') {
+        const int k = atoi(c + 3), pass = c[1] - '0';
+        if (k == 1 || k == (pass == 1 ? 3 : 2)) p->split[pass] = k;
+      }
   }
+
   int dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -550,7 +573,8 @@ template <int N, int E, int T, int MB = 0> static cudaError_t p1_run(FusedPlan* 
   const size_t sm = Plan<N, E>::stages() > 1 ? col_buf_bytes<N, T>() : 0;
   cudaError_t e = set_smem(k_p1<float, N, E, T, MB>, sm);
   if (e != cudaSuccess) return e;
-  k_p1<float, N, E, T, MB><<<(unsigned)((ncols + T - 1) / T), dim3(T, G), sm, st>>>(
+  const dim3 grid((unsigned)((ncols + T - 1) / T), (unsigned)p->split[1]);
+  k_p1<float, N, E, T, MB><<<grid, dim3(T, G), sm, st>>>(
       uh, (float2*)p->A, p->f, tw);
   return launched();
 }
@@ -562,7 +586,8 @@ template <int N, int E, int T, int MB = 0> static cudaError_t p2_run(FusedPlan* 
   const size_t sm = Plan<N, E>::stages() > 1 ? col_buf_bytes<N, T>() : 0;
   cudaError_t e = set_smem(k_p2<float, N, E, T, MB>, sm);
   if (e != cudaSuccess) return e;
-  k_p2<float, N, E, T, MB><<<(unsigned)((ncols + T - 1) / T), dim3(T, G), sm, st>>>(
+  const dim3 grid((unsigned)((ncols + T - 1) / T), (unsigned)p->split[2]);
+  k_p2<float, N, E, T, MB><<<grid, dim3(T, G), sm, st>>>(
       (const float2*)p->A, (float2*)p->B, p->f, tw);
   return launched();
 }
