@@ -1005,6 +1005,14 @@ extern "C" int pf_footprint(const pf_config* c, unsigned long long* bytes) {
       mph *= m;
     }
     b += cb * d * nspec + cb * 3 * msp + rsz * d * mph + rsz * (d == 3 ? 3 : 1) * mph;
+    bool fz = d == 3 && c->precision == PF_FP32 && c->fused && c->n[2] <= 256;
+    for (int a = 0; fz && a < 3; ++a)
+      fz = c->n[a] >= 16 && c->n[a] <= 256 && (c->n[a] & (c->n[a] - 1)) == 0;
+    if (fz) {  // fused 3/2 schedule: pass buffers on the padded x0 (and x1) grid
+      const unsigned long long t0 = 3ull * c->n[0] / 2, t1 = 3ull * c->n[1] / 2;
+      const unsigned long long nh = c->n[2] / 2 + 1;
+      b += cb * (5ull * t0 * c->n[1] * nh + 6ull * t0 * t1 * nh + 3ull * t0 * t1 * nh);
+    }
   } else if (c->is_nonlinear) {
     b += cb * d * nspec + rsz * d * nphys + rsz * (d == 3 ? 3 : 1) * nphys;
     bool pow2 = d == 3 && c->precision == PF_FP32 && c->fused && c->n[2] <= 256;

@@ -27,27 +27,32 @@
 
 namespace pf {
 
+// Transform lengths are 2^b (2/3 rule) or 3 * 2^b (3/2 rule, M = 3n/2); a
+// radix-3 first stage needs E divisible by 3.
 template <int N> struct TuneS {  // strided passes P1, P2, P4 (T measured best at 128 / G)
-  static constexpr int E = N <= 16 ? N : (N <= 64 ? 8 : 16);
+  static constexpr int E = N % 3 == 0 ? 12 : (N <= 16 ? N : (N <= 64 ? 8 : 16));
   static constexpr int G = N / E;
   static constexpr int T = (128 / G) < 8 ? 8 : ((128 / G) > 64 ? 64 : 128 / G);
 };
 template <int N> struct TuneU {  // P5 (FFT + update, three fields staged in smem)
-  static constexpr int E = N <= 16 ? N : (N <= 64 ? 8 : 16);
+  static constexpr int E = TuneS<N>::E;
   static constexpr int G = N / E;
-  static constexpr int T = (256 / G) < 4 ? 4 : ((256 / G) > 64 ? 64 : 256 / G);
+  static constexpr int T0 = (256 / G) < 4 ? 4 : ((256 / G) > 64 ? 64 : 256 / G);
+  // 3 * 2^b: the staging tile (3 N T values) kept near 100 KB
+  static constexpr int T = (N % 3 == 0 && 24 * N * T0 > 100 * 1024) ? T0 / 2 : T0;
 };
-template <int N> struct TuneC {  // contiguous pass P3: 8 values per lane
-  static constexpr int E = 8;
-  static constexpr int G = N / E;   // lanes per line pair, <= 32 for N <= 256
+template <int N> struct TuneC {  // contiguous pass P3: 8 (2^b) or 12 (3 * 2^b) values per lane
+  static constexpr int E = N % 3 == 0 ? 12 : 8;
+  static constexpr int G = N / E;   // lanes per line pair, <= 32 for N <= 256 / 384
   static constexpr int PW = 32 / G; // line pairs per warp
   static constexpr int W = 8;       // warps per CTA
   // exchange buffer of one line pair (8-byte values): position p lives at
   // p ^ ((p >> 3) & 15), which spreads the radix-8 stage stores (stride 8)
   // over all banks; the pair stride shifts neighbouring pairs' banks.  The
-  // sides up to 16 use a plain +1 per 16 padding instead.
-  static constexpr int BUF = N <= 16 ? N + 2 : (N == 32 ? N + 4 : (N == 64 ? N + 8 : N));
-  static PF_HD int sw(int p) { return N <= 16 ? p + (p >> 4) : p ^ ((p >> 3) & 15); }
+  // sides up to 16 and 3 * 2^b use a plain +1 per 16 padding instead.
+  static constexpr bool PLAIN = N <= 16 || N % 3 == 0;
+  static constexpr int BUF = PLAIN ? N + (N >> 4) + 1 : (N == 32 ? N + 4 : (N == 64 ? N + 8 : N));
+  static PF_HD int sw(int p) { return PLAIN ? p + (p >> 4) : p ^ ((p >> 3) & 15); }
 };
 
 // Exchange buffer of the strided passes: position p of column t.  Eight
@@ -60,20 +65,51 @@ template <int N, int T> constexpr size_t col_buf_bytes() {
 }
 
 struct FGeo {
-  int n0, n1, n2, nh;
-  int c1, c2;
+  int n0, n1, n2, nh;          // N grid (the state's grid)
+  int t0, t1, t2;              // transform lengths: n_i (2/3 rule) or 3 n_i / 2 (3/2 rule)
+  int c1, c2;                  // compact inverse-input extents along axes 1, 2
   int kmax0, kmax1, kmax2;
   double ks0, ks1, ks2;
   double cflw0, cflw1, cflw2;  // n_i / L_i
   long long nspec;
+  int nlrow;                   // nl row stride along axis 0 (t1 nh)
+  long long nlcomp;            // nl component stride (t0 t1 nh)
 };
+
+// Row i of a length-t inverse transform along an axis whose N-grid side is n:
+// its weight (0, 1/2 or 1) and the N-grid wavenumber index kf of its input.
+// 2/3 rule (PAD false, t == n): rows with |k| <= kmax are kept.  3/2 rule
+// (PAD true, t = 3n/2): the N-grid spectrum embedded in the t grid, the even
+// side's Nyquist row (wavenumber -n/2) split half to +n/2 and half to -n/2
+// (basis.py:133-134 padding).  Its N-grid row index is kf mod n.
+template <bool PAD> PF_D float row_weight(int i, int t, int n, int kmax, int& kf) {
+  if constexpr (!PAD) {
+    kf = kfreq(i, t);
+    return abs(kf) <= kmax ? 1.f : 0.f;
+  } else {
+    const int h = n >> 1, k = kfreq(i, t);
+    if (abs(k) < h) { kf = k; return 1.f; }
+    kf = -h;
+    return abs(k) == h ? 0.5f : 0.f;
+  }
+}
+
+// Forward direction of the 3/2 rule: N-grid row i of a complex axis takes
+// transform row src, plus row t - n/2 for the Nyquist row (the +n/2 and -n/2
+// wavenumbers fold into one).
+PF_D int fold_src(int i, int t, int n) {
+  const int h = n >> 1;
+  return i <= h ? i : t - (n - i);
+}
 
 struct FusedPlan {
   Geo g;
   FGeo f;
   int prec;
-  void* A = nullptr;  // 5 * n0 * c1 * c2 complex
-  void* B = nullptr;  // 6 * n0 * n1 * c2 complex
+  void* A = nullptr;  // 5 * t0 * c1 * c2 complex
+  void* B = nullptr;  // 6 * t0 * t1 * c2 complex
+  void* nlM = nullptr;  // 3/2 rule: 3 * t0 * t1 * nh complex (nl on the padded x0, x1 grid)
+  bool pad = false;
   int* err = nullptr; // device error word (bounded waits that gave up)
   int nsm = 148;
   // launch variant per pass (used where that pass's axis has 256 points):
@@ -86,7 +122,7 @@ struct FusedPlan {
 };
 
 // ---------------------------------------------------------------------- P1
-template <typename R, int N, int E, int T, int MB>
+template <typename R, int N, int E, int T, int MB, bool PAD>
 __global__ void __launch_bounds__(T * (N / E), MB)
 k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
      const cx<R>* __restrict__ tw) {
@@ -111,15 +147,30 @@ k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
   const int fs_in = (int)f.nspec;
   auto smf = [&](int pos) -> C& { return sm[col_pos<T>(pos, t)]; };
   auto sync = [] { __syncthreads(); };
-  // row e of the column: kept when |k0| <= kmax0 (recomputed, not stored)
-  auto kept = [&](int e) { return active && abs(kfreq(j + G * e, N)) <= f.kmax0; };
+  // row e of the column: weight, N-grid wavenumber index and source row
+  // (recomputed, not stored)
+  auto rowin = [&](int e, int& kf, int& src) {
+    const float w = active ? row_weight<PAD>(j + G * e, N, f.n0, f.kmax0, kf) : 0.f;
+    src = PAD ? (kf < 0 ? kf + f.n0 : kf) : j + G * e;
+    return w;
+  };
+  auto load = [&](int c, int e, int& kf) {
+    int src;
+    const float w = rowin(e, kf, src);
+    C z = w != 0.f ? uh[c * fs_in + src * row_in + in_off] : czero<C>();
+    if constexpr (PAD) z = cscale(z, (R)w);
+    return z;
+  };
   // gridDim.y == 3: block row y transforms field y alone (u0; u1 and D1;
   // u2 and D2), which triples the CTAs without extra traffic
   const int part = gridDim.y == 1 ? -1 : (int)blockIdx.y;
   C v[E], w[E];
   if (part <= 0) {
 #pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = kept(e) ? uh[(j + G * e) * row_in + in_off] : czero<C>();
+    for (int e = 0; e < E; ++e) {
+      int kf;
+      v[e] = load(0, e, kf);
+    }
     fft<N, E, +1>(v, j, tw, smf, sync);
     if (active) {
 #pragma unroll
@@ -131,8 +182,9 @@ k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
     if (part >= 0 && part != c) continue;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-      v[e] = kept(e) ? uh[c * fs_in + (j + G * e) * row_in + in_off] : czero<C>();
-      w[e] = cmuli(cscale(v[e], (R)(f.ks0 * kfreq(j + G * e, N))));
+      int kf;
+      v[e] = load(c, e, kf);
+      w[e] = cmuli(cscale(v[e], (R)(f.ks0 * kf)));
     }
     fft<N, E, +1>(v, j, tw, smf, sync);
     fft<N, E, +1>(w, j, tw, smf, sync);
@@ -147,7 +199,7 @@ k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
 }
 
 // ---------------------------------------------------------------------- P2
-template <typename R, int N, int E, int T, int MB>
+template <typename R, int N, int E, int T, int MB, bool PAD>
 __global__ void __launch_bounds__(T * (N / E), MB)
 k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
      const cx<R>* __restrict__ tw) {
@@ -156,7 +208,7 @@ k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   const int t = threadIdx.x, j = threadIdx.y;
-  const int ncols = f.n0 * f.c2;
+  const int ncols = f.t0 * f.c2;
   const int q = blockIdx.x * T + t;
   const bool active = q < ncols;
   int in_base = 0, out_base = 0;
@@ -168,17 +220,34 @@ k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
     out_base = x0 * N * f.c2 + k2c;
     k2 = (R)(f.ks2 * k2c);
   }
-  const int fs_in = f.n0 * f.c1 * f.c2;
-  const int fs_out = f.n0 * N * f.c2;
+  const int fs_in = f.t0 * f.c1 * f.c2;
+  const int fs_out = f.t0 * N * f.c2;
   auto smf = [&](int pos) -> C& { return sm[col_pos<T>(pos, t)]; };
   auto sync = [] { __syncthreads(); };
-  // per element e of the line (recomputed, not stored): kept flag, k1,
-  // offset of the compact input index
-  auto kept = [&](int e) { return active && abs(kfreq(j + G * e, N)) <= f.kmax1; };
-  auto k1 = [&](int e) { return (R)(f.ks1 * kfreq(j + G * e, N)); };
-  auto off = [&](int e) {
-    const int i1 = j + G * e;
-    return in_base + (i1 <= f.kmax1 ? i1 : i1 - (N - f.c1)) * f.c2;
+  // per element e of the line (recomputed, not stored): weight, k1 and the
+  // compact input row
+  auto wt = [&](int e, int& kf) {
+    return active ? row_weight<PAD>(j + G * e, N, f.n1, f.kmax1, kf) : 0.f;
+  };
+  auto k1 = [&](int e) {
+    int kf;
+    wt(e, kf);
+    return (R)(f.ks1 * kf);
+  };
+  auto ld = [&](int fld, int e) {
+    int kf;
+    const float w = wt(e, kf);
+    if (w == 0.f) return czero<C>();
+    int row;
+    if constexpr (PAD) {
+      row = kf < 0 ? kf + f.n1 : kf;
+    } else {
+      const int i1 = j + G * e;
+      row = i1 <= f.kmax1 ? i1 : i1 - (N - f.c1);
+    }
+    C z = A[fld * fs_in + in_base + row * f.c2];
+    if constexpr (PAD) z = cscale(z, (R)w);
+    return z;
   };
   auto store = [&](int fld, const C (&v)[E]) {
     if (active) {
@@ -194,9 +263,8 @@ k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
     // omega0 = i (k1 u2 - k2 u1); u1; u2
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-      const bool kp = kept(e);
-      a[e] = kp ? A[1 * fs_in + off(e)] : czero<C>();
-      b[e] = kp ? A[2 * fs_in + off(e)] : czero<C>();
+      a[e] = ld(1, e);
+      b[e] = ld(2, e);
       w[e] = cmuli(csub(cscale(b[e], k1(e)), cscale(a[e], k2)));
     }
     fft<N, E, +1>(w, j, tw, smf, sync);
@@ -210,16 +278,15 @@ k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
     // omega2 = D1 - i k1 u0; omega1 = i k2 u0 - D2; u0
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-      const bool kp = kept(e);
-      a[e] = kp ? A[0 * fs_in + off(e)] : czero<C>();
-      b[e] = kp ? A[3 * fs_in + off(e)] : czero<C>();
+      a[e] = ld(0, e);
+      b[e] = ld(3, e);
       w[e] = csub(b[e], cmuli(cscale(a[e], k1(e))));
     }
     fft<N, E, +1>(w, j, tw, smf, sync);
     store(5, w);
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-      b[e] = kept(e) ? A[4 * fs_in + off(e)] : czero<C>();
+      b[e] = ld(4, e);
       w[e] = csub(cmuli(cscale(a[e], k2)), b[e]);
     }
     fft<N, E, +1>(w, j, tw, smf, sync);
@@ -360,7 +427,7 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
         const int k = j + G * e;
         if (k <= H) {
           const C zk = smf(k);
-          const C zn = smf((N - k) & (N - 1));
+          const C zn = smf(k == 0 ? 0 : N - k);
           C Av, Bv;
           Av.x = (zk.x + zn.x) * h; Av.y = (zk.y - zn.y) * h;
           Bv.x = (zk.y + zn.y) * h; Bv.y = -(zk.x - zn.x) * h;
@@ -378,10 +445,168 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
   }
 }
 
+// P3 of the 3/2 rule: padded lines of t2 = 3 n2 / 2 points, inputs k2 <= n2/2
+// (the Nyquist column halved), outputs k2 <= n2/2 (the Nyquist entry plus its
+// -n2/2 partner, the conjugate).  Twelve values per lane and six fields would
+// not fit the registers, so u goes to thread-private shared-memory slots
+// after its C2R and omega is transformed one field at a time, accumulating
+// u x omega in registers.  One staging buffer per warp, refilled once the
+// group's last field is in registers.
+template <typename R, int N, int W>
+__global__ void __launch_bounds__(32 * W, 1)
+k_p3pad(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
+        const cx<R>* __restrict__ tw, unsigned long long* __restrict__ maxbits, R scale,
+        int* __restrict__ err, long long ngroups) {
+  constexpr int E = TuneC<N>::E, G = TuneC<N>::G, PW = TuneC<N>::PW;
+  constexpr int H = N / 2;
+  constexpr int BUF = TuneC<N>::BUF;
+  static_assert(G <= 32 && 32 % G == 0, "line pairs tile a warp");
+  static_assert(W <= 16, "mbarriers fit the 128-byte header");
+  using C = cx<R>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int pw = lane / G, j = lane % G;
+  const int fb = 2 * PW * f.c2;
+  const int SC = 6 * fb;
+  const int WC = ((SC + PW * BUF + PW * 3 * N) + 15) & ~15;
+  const uint32_t fbytes = (uint32_t)(fb * sizeof(C));
+  const long long fs_in = (long long)f.t0 * f.t1 * f.c2;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smraw) + warp;
+  C* wbase = reinterpret_cast<C*>(smraw + 128) + (long long)warp * WC;
+  C* ex = wbase + SC + pw * BUF;
+  C* ur = wbase + SC + PW * BUF + pw * 3 * N;  // u on the padded line, own slots
+  if (lane == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+  auto issue = [&](long long grp) {
+    if (lane == 0) {
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(bar, 6 * fbytes);
+      const C* src = B + grp * fb;
+#pragma unroll
+      for (int fld = 0; fld < 6; ++fld) bulk_g2s(wbase + fld * fb, src + fld * fs_in, fbytes, bar);
+    }
+  };
+  auto smf = [&](int pos) -> C& { return ex[TuneC<N>::sw(pos)]; };
+  auto sync = [] { __syncwarp(); };
+  auto unpack = [&](const C* pa, C (&z)[E]) {
+    const C* pb = pa + f.c2;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int m = j + G * e;
+      const int k = m <= H ? m : N - m;
+      const bool kin = k < f.c2;
+      C a = kin ? pa[k] : czero<C>();
+      C b = kin ? pb[k] : czero<C>();
+      if (k == f.c2 - 1) { a = cscale(a, R(0.5)); b = cscale(b, R(0.5)); }
+      if (m == 0) { a.y = 0; b.y = 0; }
+      C r;
+      if (m <= H) { r.x = a.x - b.y; r.y = a.y + b.x; }
+      else { r.x = a.x + b.y; r.y = b.x - a.y; }
+      z[e] = r;
+    }
+  };
+  // line a in the real parts, line b in the imaginary parts
+  auto mul = [](C p, C q) { C r; r.x = p.x * q.x; r.y = p.y * q.y; return r; };
+  const long long TW = (long long)gridDim.x * W;
+  long long g = (long long)blockIdx.x * W + warp;
+  if (g < ngroups) issue(g);
+  double mx = 0.0;
+  const R h = R(0.5) * scale;
+  for (int it = 0; g < ngroups; g += TW, ++it) {
+    const bool more = g + TW < ngroups;
+    const bool ok = mbar_wait_bounded(bar, (uint32_t)(it & 1));
+    if (!__all_sync(0xffffffffu, ok)) {
+      if (lane == 0) atomicExch(err, kErrWaitP3);
+      return;
+    }
+    const C* in = wbase + 2 * pw * f.c2;
+    C v[E];
+#pragma unroll
+    for (int fld = 0; fld < 3; ++fld) {
+      unpack(in + fld * fb, v);
+      fft<N, E, +1>(v, j, tw, smf, sync);
+#pragma unroll
+      for (int e = 0; e < E; ++e) ur[fld * N + j + G * e] = v[e];
+    }
+    if (maxbits) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const C u0 = ur[j + G * e], u1 = ur[N + j + G * e], u2 = ur[2 * N + j + G * e];
+        const double sa = fabs((double)u0.x) * f.cflw0 + fabs((double)u1.x) * f.cflw1 +
+                          fabs((double)u2.x) * f.cflw2;
+        const double sb = fabs((double)u0.y) * f.cflw0 + fabs((double)u1.y) * f.cflw1 +
+                          fabs((double)u2.y) * f.cflw2;
+        mx = fmax(mx, fmax(sa, sb));
+      }
+    }
+    C c[3][E];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int e = 0; e < E; ++e) c[i][e] = czero<C>();
+#pragma unroll
+    for (int wc = 0; wc < 3; ++wc) {
+      unpack(in + (3 + wc) * fb, v);
+      if (wc == 2) {
+        __syncwarp();  // every lane has read the group
+        if (more) issue(g + TW);
+      }
+      fft<N, E, +1>(v, j, tw, smf, sync);
+      // c0 = u1 w2 - u2 w1, c1 = u2 w0 - u0 w2, c2 = u0 w1 - u1 w0: field wc
+      // adds u[wc+2] w to c[wc+1] and subtracts u[wc+1] w from c[wc+2]
+      const int ia = (wc + 1) % 3, ib = (wc + 2) % 3;
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const C ua = ur[ia * N + j + G * e], ub = ur[ib * N + j + G * e];
+        c[ia][e] = cadd(c[ia][e], mul(ub, v[e]));
+        c[ib][e] = csub(c[ib][e], mul(ua, v[e]));
+      }
+    }
+    const long long la = 2 * (g * PW + pw);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      fft<N, E, -1>(c[i], j, tw, smf, sync);
+#pragma unroll
+      for (int e = 0; e < E; ++e) smf(j + G * e) = c[i][e];
+      sync();
+      C* oa = nl + i * f.nlcomp + la * f.nh;
+      C* ob = oa + f.nh;
+#pragma unroll
+      for (int e = 0; e <= E / 2; ++e) {
+        const int k = j + G * e;
+        if (k < f.nh) {
+          const C zk = smf(k);
+          const C zn = smf(k == 0 ? 0 : N - k);
+          C Av, Bv;
+          Av.x = (zk.x + zn.x) * h; Av.y = (zk.y - zn.y) * h;
+          Bv.x = (zk.y + zn.y) * h; Bv.y = -(zk.x - zn.x) * h;
+          if (k == f.nh - 1) {
+            Av.x *= R(2); Av.y = R(0);
+            Bv.x *= R(2); Bv.y = R(0);
+          }
+          oa[k] = Av;
+          ob[k] = Bv;
+        }
+      }
+      sync();
+    }
+  }
+  if (maxbits) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) atomicMax(maxbits, (unsigned long long)__double_as_longlong(mx));
+  }
+}
+
 // ---------------------------------------------------------------------- P4
 // In-place forward FFT along axis 1 of nl[3][x0][x1][k2]: column q = (plane,
-// k2) with plane = comp * n0 + x0.
-template <typename R, int N, int E, int T, int MB>
+// k2) with plane = comp * t0 + x0.  3/2 rule: the t1 transform rows are then
+// truncated to the n1 N-grid rows (+n1/2 and -n1/2 folded into the Nyquist
+// row), written to the first n1 rows of the column.
+template <typename R, int N, int E, int T, int MB, bool PAD>
 __global__ void __launch_bounds__(T * (N / E), MB)
 k_p4(cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
   constexpr int G = N / E;
@@ -389,7 +614,7 @@ k_p4(cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
   const int t = threadIdx.x, j = threadIdx.y;
-  const long long ncols = (long long)3 * f.n0 * f.nh;
+  const long long ncols = (long long)3 * f.t0 * f.nh;
   const long long q = (long long)blockIdx.x * T + t;
   const bool active = q < ncols;
   long long base = 0;
@@ -403,9 +628,27 @@ k_p4(cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
     v[e] = active ? nl[base + (long long)(j + G * e) * f.nh] : czero<C>();
   fft<N, E, -1>(v, j, tw, [&](int pos) -> C& { return sm[col_pos<T>(pos, t)]; },
                 [] { __syncthreads(); });
-  if (active) {
+  if constexpr (!PAD) {
+    if (active) {
 #pragma unroll
-    for (int e = 0; e < E; ++e) nl[base + (long long)(j + G * e) * f.nh] = v[e];
+      for (int e = 0; e < E; ++e) nl[base + (long long)(j + G * e) * f.nh] = v[e];
+    }
+  } else {
+    // the FFT's last exchange was read before its closing barrier
+#pragma unroll
+    for (int e = 0; e < E; ++e) sm[col_pos<T>(j + G * e, t)] = v[e];
+    __syncthreads();
+    constexpr int EU = 2 * E / 3;  // n1 = 2 N / 3 rows, G per step
+    const int h = f.n1 >> 1;
+    if (active) {
+#pragma unroll
+      for (int e = 0; e < EU; ++e) {
+        const int i = j + G * e;
+        C z = sm[col_pos<T>(fold_src(i, N, f.n1), t)];
+        if (i == h) z = cadd(z, sm[col_pos<T>(N - h, t)]);
+        nl[base + (long long)i * f.nh] = z;
+      }
+    }
   }
 }
 
@@ -414,7 +657,7 @@ k_p4(cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
 // N x T buffer per component, also the FFT's exchange buffer) so the update
 // phase holds only a chunk of modes in registers; u_hat / u0 of a chunk are
 // loaded before any of its stores.
-template <typename R, int N, int NC, bool NOISE, int CHU>
+template <typename R, int N, int NC, bool NOISE, int CHU, bool PAD>
 __global__ void __launch_bounds__(TuneU<N>::T * TuneU<N>::G, 2)
 k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
   constexpr int E = TuneU<N>::E, G = TuneU<N>::G, T = TuneU<N>::T;
@@ -426,12 +669,12 @@ k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restr
   const int ncols = f.n1 * f.nh;
   const int q = blockIdx.x * T + t;
   const bool active = q < ncols;
-  const int fs = (int)f.nspec;
+  const long long fs = f.nlcomp;  // nl: [3][t0][rows of nlrow]; 2/3 rule: the state layout
   auto sync = [] { __syncthreads(); };
   // component c + 1 is loaded while component c is transformed
   C v[E], nx[E];
 #pragma unroll
-  for (int e = 0; e < E; ++e) nx[e] = active ? nl[(j + G * e) * ncols + q] : czero<C>();
+  for (int e = 0; e < E; ++e) nx[e] = active ? nl[(j + G * e) * f.nlrow + q] : czero<C>();
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     C* Sc = S + c * N * T;
@@ -441,12 +684,28 @@ k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restr
     if (c < 2) {
 #pragma unroll
       for (int e = 0; e < E; ++e)
-        nx[e] = active ? nl[(c + 1) * fs + (j + G * e) * ncols + q] : czero<C>();
+        nx[e] = active ? nl[(c + 1) * fs + (j + G * e) * f.nlrow + q] : czero<C>();
     }
     fft<N, E, -1>(v, j, tw, smf, sync);
 #pragma unroll
     for (int e = 0; e < E; ++e) Sc[(j + G * e) * T + t] = v[e];
   }
+  // 3/2 rule: the update reads the folded rows, written by other threads
+  if constexpr (PAD) __syncthreads();
+  // N-grid rows per thread: all E (2/3 rule) or the n0 = 2N/3 of the t0 = N
+  // transform rows (3/2 rule)
+  constexpr int EU = PAD ? 2 * E / 3 : E;
+  static_assert(EU % CH == 0, "whole chunks of rows");
+  const int h0 = f.n0 >> 1;
+  auto nhat = [&](int a, int i0) {
+    if constexpr (!PAD) {
+      return S[a * N * T + i0 * T + t];
+    } else {
+      C z = S[a * N * T + fold_src(i0, N, f.n0) * T + t];
+      if (i0 == h0) z = cadd(z, S[a * N * T + (N - h0) * T + t]);
+      return z;
+    }
+  };
   const StageScalars<R> sc = stage_scalars<R>(U);
   double accE = 0.0, accZ = 0.0;
   if (active) {
@@ -456,7 +715,7 @@ k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restr
     const cx<R>* __restrict__ u0p = U.u0;
     const long long ns = f.nspec;
 #pragma unroll
-    for (int e0 = 0; e0 < E; e0 += CH) {
+    for (int e0 = 0; e0 < EU; e0 += CH) {
       C un[CH][3], u0v[CH][3];
 #pragma unroll
       for (int cc = 0; cc < CH; ++cc) {
@@ -473,12 +732,12 @@ k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restr
         const long long m = (long long)i0 * ncols + q;
         ModeK<R, 3> mk_;
         mk_.ix.i0 = i0; mk_.ix.i1 = i1; mk_.ix.i2 = i2;
-        const R k0 = (R)(f.ks0 * kfreq(i0, N));
+        const R k0 = (R)(f.ks0 * kfreq(i0, f.n0));
         mk_.k[0] = k0; mk_.k[1] = k1; mk_.k[2] = k2;
         mk_.k2 = k0 * k0 + k1 * k1 + k2 * k2;
         C nv[3];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) nv[a] = S[a * N * T + i0 * T + t];
+        for (int a = 0; a < 3; ++a) nv[a] = nhat(a, i0);
         update_core<R, 3, NC, NOISE>(U, m, mk_, nv, true, un[cc], u0v[cc], sc, accE, accZ);
       }
     }
@@ -498,18 +757,31 @@ template <typename K> static cudaError_t set_smem(K kern, size_t bytes) {
 static bool pow2(int n) { return n >= 16 && (n & (n - 1)) == 0; }
 
 FusedPlan* fused_create(const Geo& g, int precision, int dealias) {
-  if (g.dim != 3 || precision != 0 || dealias != 0) return nullptr;
+  if (g.dim != 3 || precision != 0 || (dealias != 0 && dealias != 1)) return nullptr;
+  const bool pad = dealias == 1;
+  // 2/3 rule: sides 16..512 (the last up to 256); 3/2 rule: sides 16..256
+  // (transform lengths 24..384)
   for (int a = 0; a < 3; ++a)
-    if (!pow2(g.n[a]) || g.n[a] > 512) return nullptr;
+    if (!pow2(g.n[a]) || g.n[a] > (pad ? 256 : 512)) return nullptr;
   if (g.n[2] > 256) return nullptr;
   FusedPlan* p = new FusedPlan();
   p->g = g;
   p->prec = precision;
+  p->pad = pad;
   FGeo& f = p->f;
   f.n0 = g.n[0]; f.n1 = g.n[1]; f.n2 = g.n[2]; f.nh = g.nh;
   f.kmax0 = g.kmax[0]; f.kmax1 = g.kmax[1]; f.kmax2 = g.kmax[2];
-  f.c1 = 2 * f.kmax1 + 1;
-  f.c2 = f.kmax2 + 1;
+  if (pad) {
+    f.t0 = 3 * f.n0 / 2; f.t1 = 3 * f.n1 / 2; f.t2 = 3 * f.n2 / 2;
+    f.c1 = f.n1;  // every N-grid k1 and k2 feeds the padded grid
+    f.c2 = f.nh;
+  } else {
+    f.t0 = f.n0; f.t1 = f.n1; f.t2 = f.n2;
+    f.c1 = 2 * f.kmax1 + 1;
+    f.c2 = f.kmax2 + 1;
+  }
+  f.nlrow = f.t1 * f.nh;
+  f.nlcomp = (long long)f.t0 * f.t1 * f.nh;
   f.ks0 = g.kscale[0]; f.ks1 = g.kscale[1]; f.ks2 = g.kscale[2];
   f.cflw0 = g.n[0] * g.kscale[0] / (2.0 * M_PI);
   f.cflw1 = g.n[1] * g.kscale[1] / (2.0 * M_PI);
@@ -519,7 +791,8 @@ FusedPlan* fused_create(const Geo& g, int precision, int dealias) {
     // "p1:1,p2:2,p4:1"
     for (const char* c = v; *c; ++c)
       if (c[0] == 'p' && c[1] >= '1' && c[1] <= '5' && c[2] == ':') p->var[c[1] - '0'] = atoi(c + 3);
-  }  if (const char* v = getenv("PF_FUSED_SPLIT")) {
+  }
+  if (const char* v = getenv("PF_FUSED_SPLIT")) {
     for (const char* c = v; *c; ++c)
       if (c[0] == 'p' && (c[1] == '1' || c[1] == '2') && c[2] == ':') {
         const int k = atoi(c + 3), pass = c[1] - '0';
@@ -531,8 +804,9 @@ FusedPlan* fused_create(const Geo& g, int precision, int dealias) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, dev);
   const size_t cb = precision == 0 ? 8 : 16;
-  const size_t a_el = 5ull * f.n0 * f.c1 * f.c2, b_el = 6ull * f.n0 * f.n1 * f.c2;
+  const size_t a_el = 5ull * f.t0 * f.c1 * f.c2, b_el = 6ull * f.t0 * f.t1 * f.c2;
   if (cudaMalloc(&p->A, cb * a_el) != cudaSuccess || cudaMalloc(&p->B, cb * b_el) != cudaSuccess ||
+      (pad && cudaMalloc(&p->nlM, cb * (size_t)(3 * f.nlcomp)) != cudaSuccess) ||
       cudaMalloc(&p->err, sizeof(int)) != cudaSuccess ||
       cudaMemset(p->err, 0, sizeof(int)) != cudaSuccess) {
     fused_destroy(p);
@@ -546,6 +820,7 @@ void fused_destroy(FusedPlan* p) {
   if (!p) return;
   if (p->A) cudaFree(p->A);
   if (p->B) cudaFree(p->B);
+  if (p->nlM) cudaFree(p->nlM);
   if (p->err) cudaFree(p->err);
   delete p;
 }
@@ -560,78 +835,114 @@ void fused_destroy(FusedPlan* p) {
     case 512: return CALL(512);   \
     default: return cudaErrorInvalidValue; \
   }
+// transform lengths of the 3/2 rule (N-grid sides 16..256)
+#define PF_SWITCH_M(n, CALL)      \
+  switch (n) {                    \
+    case 24: return CALL(24);     \
+    case 48: return CALL(48);     \
+    case 96: return CALL(96);     \
+    case 192: return CALL(192);   \
+    case 384: return CALL(384);   \
+    default: return cudaErrorInvalidValue; \
+  }
 
 // Launch variants (radix width E, columns per CTA T, minimum CTAs per SM MB
 // that caps registers; 0: no cap) of the strided passes; variant 0 is the
 // TuneS default, 1..6 exist for n = 256 (tuning knob
 // PF_FUSED_VARIANT="p1:v,p2:v,p3:v,p4:v", which overrides FusedPlan::var).
-template <int N, int E, int T, int MB = 0> static cudaError_t p1_run(FusedPlan* p, const float2* uh,
-                                                        cudaStream_t st) {
+// The 3/2 rule always needs the exchange buffer (P4 folds through it).
+template <int N, int E, int T, int MB, bool PAD>
+constexpr size_t strided_smem() {
+  return (PAD || Plan<N, E>::stages() > 1) ? col_buf_bytes<N, T>() : 0;
+}
+
+template <bool PAD, int N, int E, int T, int MB = 0>
+static cudaError_t p1_run(FusedPlan* p, const float2* uh, cudaStream_t st) {
   constexpr int G = N / E;
   const float2* tw = tw_base<float>() + tw_offset(N);
   const long long ncols = (long long)p->f.c1 * p->f.c2;
-  const size_t sm = Plan<N, E>::stages() > 1 ? col_buf_bytes<N, T>() : 0;
-  cudaError_t e = set_smem(k_p1<float, N, E, T, MB>, sm);
+  const size_t sm = strided_smem<N, E, T, MB, PAD>();
+  cudaError_t e = set_smem(k_p1<float, N, E, T, MB, PAD>, sm);
   if (e != cudaSuccess) return e;
   const dim3 grid((unsigned)((ncols + T - 1) / T), (unsigned)p->split[1]);
-  k_p1<float, N, E, T, MB><<<grid, dim3(T, G), sm, st>>>(
-      uh, (float2*)p->A, p->f, tw);
+  k_p1<float, N, E, T, MB, PAD><<<grid, dim3(T, G), sm, st>>>(uh, (float2*)p->A, p->f, tw);
   return launched();
 }
 
-template <int N, int E, int T, int MB = 0> static cudaError_t p2_run(FusedPlan* p, cudaStream_t st) {
+template <bool PAD, int N, int E, int T, int MB = 0>
+static cudaError_t p2_run(FusedPlan* p, cudaStream_t st) {
   constexpr int G = N / E;
   const float2* tw = tw_base<float>() + tw_offset(N);
-  const long long ncols = (long long)p->f.n0 * p->f.c2;
-  const size_t sm = Plan<N, E>::stages() > 1 ? col_buf_bytes<N, T>() : 0;
-  cudaError_t e = set_smem(k_p2<float, N, E, T, MB>, sm);
+  const long long ncols = (long long)p->f.t0 * p->f.c2;
+  const size_t sm = strided_smem<N, E, T, MB, PAD>();
+  cudaError_t e = set_smem(k_p2<float, N, E, T, MB, PAD>, sm);
   if (e != cudaSuccess) return e;
   const dim3 grid((unsigned)((ncols + T - 1) / T), (unsigned)p->split[2]);
-  k_p2<float, N, E, T, MB><<<grid, dim3(T, G), sm, st>>>(
+  k_p2<float, N, E, T, MB, PAD><<<grid, dim3(T, G), sm, st>>>(
       (const float2*)p->A, (float2*)p->B, p->f, tw);
   return launched();
 }
 
-template <int N, int E, int T, int MB = 0> static cudaError_t p4_run(FusedPlan* p, float2* nl,
-                                                        cudaStream_t st) {
+template <bool PAD, int N, int E, int T, int MB = 0>
+static cudaError_t p4_run(FusedPlan* p, float2* nl, cudaStream_t st) {
   constexpr int G = N / E;
   const float2* tw = tw_base<float>() + tw_offset(N);
-  const long long ncols = (long long)3 * p->f.n0 * p->f.nh;
-  const size_t sm = Plan<N, E>::stages() > 1 ? col_buf_bytes<N, T>() : 0;
-  cudaError_t e = set_smem(k_p4<float, N, E, T, MB>, sm);
+  const long long ncols = (long long)3 * p->f.t0 * p->f.nh;
+  const size_t sm = strided_smem<N, E, T, MB, PAD>();
+  cudaError_t e = set_smem(k_p4<float, N, E, T, MB, PAD>, sm);
   if (e != cudaSuccess) return e;
-  k_p4<float, N, E, T, MB><<<(unsigned)((ncols + T - 1) / T), dim3(T, G), sm, st>>>(nl, p->f, tw);
+  k_p4<float, N, E, T, MB, PAD><<<(unsigned)((ncols + T - 1) / T), dim3(T, G), sm, st>>>(
+      nl, p->f, tw);
   return launched();
 }
 
 #define PF_VARIANTS(RUN, N, ...)                                        \
   if constexpr (N == 256) {                                             \
     switch (var) {                                                      \
-      case 1: return RUN<256, 8, 16>(__VA_ARGS__);                      \
-      case 2: return RUN<256, 8, 32>(__VA_ARGS__);                      \
-      case 3: return RUN<256, 16, 8>(__VA_ARGS__);                      \
-      case 4: return RUN<256, 16, 8, 3>(__VA_ARGS__);                   \
-      case 5: return RUN<256, 16, 8, 4>(__VA_ARGS__);                   \
-      case 6: return RUN<256, 16, 16, 2>(__VA_ARGS__);                  \
+      case 1: return RUN<PAD, 256, 8, 16>(__VA_ARGS__);                 \
+      case 2: return RUN<PAD, 256, 8, 32>(__VA_ARGS__);                 \
+      case 3: return RUN<PAD, 256, 16, 8>(__VA_ARGS__);                 \
+      case 4: return RUN<PAD, 256, 16, 8, 3>(__VA_ARGS__);              \
+      case 5: return RUN<PAD, 256, 16, 8, 4>(__VA_ARGS__);              \
+      case 6: return RUN<PAD, 256, 16, 16, 2>(__VA_ARGS__);             \
       default: break;                                                   \
     }                                                                   \
   }                                                                     \
-  return RUN<N, TuneS<N>::E, TuneS<N>::T>(__VA_ARGS__);
+  return RUN<PAD, N, TuneS<N>::E, TuneS<N>::T>(__VA_ARGS__);
 
-template <int N> static cudaError_t p1_n(FusedPlan* p, const float2* uh, cudaStream_t st) {
+template <int N, bool PAD> static cudaError_t p1_n(FusedPlan* p, const float2* uh, cudaStream_t st) {
   const int var = p->var[1];
   PF_VARIANTS(p1_run, N, p, uh, st)
 }
-template <int N> static cudaError_t p2_n(FusedPlan* p, cudaStream_t st) {
+template <int N, bool PAD> static cudaError_t p2_n(FusedPlan* p, cudaStream_t st) {
   const int var = p->var[2];
   PF_VARIANTS(p2_run, N, p, st)
 }
-template <int N> static cudaError_t p4_n(FusedPlan* p, float2* nl, cudaStream_t st) {
+template <int N, bool PAD> static cudaError_t p4_n(FusedPlan* p, float2* nl, cudaStream_t st) {
   const int var = p->var[4];
   PF_VARIANTS(p4_run, N, p, nl, st)
 }
 
-template <int N, int NB, int W, int MB>
+template <int N, int W>
+static cudaError_t p3pad_run(FusedPlan* p, float2* nl, unsigned long long* maxbits,
+                             cudaStream_t st) {
+  using TN = TuneC<N>;
+  const float2* tw = tw_base<float>() + tw_offset(N);
+  const long long ngroups = (long long)p->f.t0 * p->f.t1 / (2 * TN::PW);
+  const int fb = 2 * TN::PW * p->f.c2;
+  const int WC = ((6 * fb + TN::PW * TN::BUF + TN::PW * 3 * N) + 15) & ~15;
+  const size_t sm = 128 + sizeof(float2) * (size_t)W * WC;
+  cudaError_t e = set_smem(k_p3pad<float, N, W>, sm);
+  if (e != cudaSuccess) return e;
+  const float scale = (float)(1.0 / ((double)p->f.t0 * p->f.t1 * p->f.t2));
+  long long blocks = (ngroups + W - 1) / W;
+  if (blocks > (long long)p->nsm) blocks = p->nsm;
+  k_p3pad<float, N, W><<<(unsigned)blocks, 32 * W, sm, st>>>(
+      (const float2*)p->B, nl, p->f, tw, maxbits, scale, p->err, ngroups);
+  return launched();
+}
+
+template <bool PAD, int N, int NB, int W, int MB>
 static cudaError_t p3_run(FusedPlan* p, float2* nl, unsigned long long* maxbits, cudaStream_t st) {
   using TN = TuneC<N>;
   const float2* tw = tw_base<float>() + tw_offset(N);
@@ -652,24 +963,28 @@ static cudaError_t p3_run(FusedPlan* p, float2* nl, unsigned long long* maxbits,
 // Variant 0: two staging buffers per warp, 8 warps, one CTA per SM; 1..3
 // (n2 = 256): one staging buffer refilled as soon as the group is in
 // registers, with 8 warps x 2 CTAs, 4 warps x 3 CTAs or 8 warps x 1 CTA.
-template <int N>
+// 3/2 rule: k_p3pad, 8 warps.
+template <int N, bool PAD>
 static cudaError_t p3_n(FusedPlan* p, float2* nl, unsigned long long* maxbits, cudaStream_t st) {
-  if constexpr (N > 256) {
+  if constexpr (PAD) {
+    if constexpr (N > 384) return cudaErrorInvalidValue;
+    else return p3pad_run<N, 8>(p, nl, maxbits, st);
+  } else if constexpr (N > 256) {
     return cudaErrorInvalidValue;
   } else {
     if constexpr (N == 256) {
       switch (p->var[3]) {
-        case 1: return p3_run<256, 1, 8, 2>(p, nl, maxbits, st);
-        case 2: return p3_run<256, 1, 4, 3>(p, nl, maxbits, st);
-        case 3: return p3_run<256, 1, 8, 1>(p, nl, maxbits, st);
+        case 1: return p3_run<PAD, 256, 1, 8, 2>(p, nl, maxbits, st);
+        case 2: return p3_run<PAD, 256, 1, 4, 3>(p, nl, maxbits, st);
+        case 3: return p3_run<PAD, 256, 1, 8, 1>(p, nl, maxbits, st);
         default: break;
       }
     }
-    return p3_run<N, 2, TuneC<N>::W, 1>(p, nl, maxbits, st);
+    return p3_run<PAD, N, 2, TuneC<N>::W, 1>(p, nl, maxbits, st);
   }
 }
 
-template <int N, int CH>
+template <bool PAD, int N, int CH>
 static cudaError_t p5_run(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, const float2* nl,
                           cudaStream_t st) {
   using TN = TuneU<N>;
@@ -679,57 +994,86 @@ static cudaError_t p5_run(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, c
   const dim3 grid((unsigned)((ncols + TN::T - 1) / TN::T)), block(TN::T, TN::G);
   cudaError_t e;
   if (U.noise_src == kNoiseNone) {
-    e = set_smem(k_p5<float, N, 3, false, CH>, sm);
+    e = set_smem(k_p5<float, N, 3, false, CH, PAD>, sm);
     if (e != cudaSuccess) return e;
-    k_p5<float, N, 3, false, CH><<<grid, block, sm, st>>>(U, nl, p->f, tw);
+    k_p5<float, N, 3, false, CH, PAD><<<grid, block, sm, st>>>(U, nl, p->f, tw);
   } else if (ncomp == 9) {
-    e = set_smem(k_p5<float, N, 9, true, CH>, sm);
+    e = set_smem(k_p5<float, N, 9, true, CH, PAD>, sm);
     if (e != cudaSuccess) return e;
-    k_p5<float, N, 9, true, CH><<<grid, block, sm, st>>>(U, nl, p->f, tw);
+    k_p5<float, N, 9, true, CH, PAD><<<grid, block, sm, st>>>(U, nl, p->f, tw);
   } else {
-    e = set_smem(k_p5<float, N, 3, true, CH>, sm);
+    e = set_smem(k_p5<float, N, 3, true, CH, PAD>, sm);
     if (e != cudaSuccess) return e;
-    k_p5<float, N, 3, true, CH><<<grid, block, sm, st>>>(U, nl, p->f, tw);
+    k_p5<float, N, 3, true, CH, PAD><<<grid, block, sm, st>>>(U, nl, p->f, tw);
   }
   return launched();
 }
 
 // Variant 0 keeps the state loads of 4 rows per thread in flight; 1, 2
 // (n0 = 256) use 2 and 8.
-template <int N>
+template <int N, bool PAD>
 static cudaError_t p5_n(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, const float2* nl,
                         cudaStream_t st) {
   if constexpr (N == 256) {
     switch (p->var[5]) {
-      case 1: return p5_run<256, 2>(p, U, ncomp, nl, st);
-      case 2: return p5_run<256, 8>(p, U, ncomp, nl, st);
+      case 1: return p5_run<PAD, 256, 2>(p, U, ncomp, nl, st);
+      case 2: return p5_run<PAD, 256, 8>(p, U, ncomp, nl, st);
       default: break;
     }
   }
-  return p5_run<N, 4>(p, U, ncomp, nl, st);
+  return p5_run<PAD, N, 4>(p, U, ncomp, nl, st);
 }
 
+// 2/3 rule: nl is the caller's buffer in the state layout; 3/2 rule: passes 3
+// and 4 work in the plan's padded-grid buffer, which pass 5 reads.
 cudaError_t fused_pass(FusedPlan* p, int pass, const void* uhat, void* nl,
                        unsigned long long* maxbits, cudaStream_t st) {
   if (!p || !tw_base<float>()) return cudaErrorNotReady;
+  float2* nlp = p->pad ? (float2*)p->nlM : (float2*)nl;
+  if (p->pad) {
+    switch (pass) {
+      case 1: {
+#define PF_CALL(NN) p1_n<NN, true>(p, (const float2*)uhat, st)
+        PF_SWITCH_M(p->f.t0, PF_CALL)
+#undef PF_CALL
+      }
+      case 2: {
+#define PF_CALL(NN) p2_n<NN, true>(p, st)
+        PF_SWITCH_M(p->f.t1, PF_CALL)
+#undef PF_CALL
+      }
+      case 3: {
+#define PF_CALL(NN) p3_n<NN, true>(p, nlp, maxbits, st)
+        PF_SWITCH_M(p->f.t2, PF_CALL)
+#undef PF_CALL
+      }
+      case 4: {
+#define PF_CALL(NN) p4_n<NN, true>(p, nlp, st)
+        PF_SWITCH_M(p->f.t1, PF_CALL)
+#undef PF_CALL
+      }
+      default:
+        return cudaErrorInvalidValue;
+    }
+  }
   switch (pass) {
     case 1: {
-#define PF_CALL(NN) p1_n<NN>(p, (const float2*)uhat, st)
+#define PF_CALL(NN) p1_n<NN, false>(p, (const float2*)uhat, st)
       PF_SWITCH_S(p->f.n0, PF_CALL)
 #undef PF_CALL
     }
     case 2: {
-#define PF_CALL(NN) p2_n<NN>(p, st)
+#define PF_CALL(NN) p2_n<NN, false>(p, st)
       PF_SWITCH_S(p->f.n1, PF_CALL)
 #undef PF_CALL
     }
     case 3: {
-#define PF_CALL(NN) p3_n<NN>(p, (float2*)nl, maxbits, st)
+#define PF_CALL(NN) p3_n<NN, false>(p, nlp, maxbits, st)
       PF_SWITCH_S(p->f.n2, PF_CALL)
 #undef PF_CALL
     }
     case 4: {
-#define PF_CALL(NN) p4_n<NN>(p, (float2*)nl, st)
+#define PF_CALL(NN) p4_n<NN, false>(p, nlp, st)
       PF_SWITCH_S(p->f.n1, PF_CALL)
 #undef PF_CALL
     }
@@ -741,7 +1085,12 @@ cudaError_t fused_pass(FusedPlan* p, int pass, const void* uhat, void* nl,
 cudaError_t fused_update(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, const void* nl,
                          cudaStream_t st) {
   if (!p || !tw_base<float>()) return cudaErrorNotReady;
-#define PF_CALL(NN) p5_n<NN>(p, U, ncomp, (const float2*)nl, st)
+  if (p->pad) {
+#define PF_CALL(NN) p5_n<NN, true>(p, U, ncomp, (const float2*)p->nlM, st)
+    PF_SWITCH_M(p->f.t0, PF_CALL)
+#undef PF_CALL
+  }
+#define PF_CALL(NN) p5_n<NN, false>(p, U, ncomp, (const float2*)nl, st)
   PF_SWITCH_S(p->f.n0, PF_CALL)
 #undef PF_CALL
 }
