@@ -141,11 +141,11 @@ def oracle_initial_field(n, seed):
     return O.spectral_random_field(O.Grid((n, n, n)), seed)
 
 
-def make_solver(n, precision="fp32"):
+def make_solver(n, precision="fp32", dealias="2/3", fused=True):
     from periodicflow import simulation as sim
     return sim.Solver([n] * 3, CFG["dt0"], 1.0, time_integrator=CFG["integrator"],
-                      viscosity=CFG["nu"], dealias="2/3", precision=precision,
-                      forcing=CFG["forcing"], cfl=CFG["cfl"])
+                      viscosity=CFG["nu"], dealias=dealias, precision=precision,
+                      forcing=CFG["forcing"], cfl=CFG["cfl"], fused=fused)
 
 
 def run_ours(args, dist, rank, world):
@@ -228,6 +228,9 @@ def run_ours(args, dist, rank, world):
     ensemble = None
     if rank == 0 and not args.no_ensemble:
         ensemble = run_ensemble(args)
+    padded = None
+    if rank == 0 and not args.no_padded:
+        padded = run_padded(args, uh0, peak)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -242,7 +245,7 @@ def run_ours(args, dist, rank, world):
                        "dt_after_run": dt_now},
             "gpu_launches": int(c1.value - c0.value),
             "clocks": ck, "roofline": roofline, "step_roofline": step_roof,
-            "e2e": e2e, "cpu_baseline": cpu, "batched": ensemble,
+            "e2e": e2e, "cpu_baseline": cpu, "batched": ensemble, "padded_3_2": padded,
         }
         print(json.dumps(line), flush=True)
 
@@ -304,6 +307,54 @@ def ensemble_members(scale=1.0, precision="fp32"):
                        dealias="2/3", precision=precision, seed=seed)
         s.set_correlation_function(np.exp(-s.space_solver.k2 / 64.0))
         out.append(s)
+    return out
+
+
+def padded_stage_bytes(n):
+    """Algorithmic bytes per stage of the fused 3/2 schedule (t = 3n/2):
+    P1 u_hat (3 U) in, A (5 t n nh) out; P2 A in, B (6 t^2 nh) out; P3 B in,
+    nl (3 t^2 nh) out; P4 nl in, folded (3 t n nh) out; P5 that in, u_hat and
+    u0 in, u_hat out.  76.5 U per stage."""
+    nh = n // 2 + 1
+    t = 3 * n // 2
+    cb = 8
+    U = n * n * nh * cb
+    A = 5 * t * n * nh * cb
+    B = 6 * t * t * nh * cb
+    NL = 3 * t * t * nh * cb
+    F = 3 * t * n * nh * cb
+    return (3 * U + A) + (A + B) + (B + NL) + (NL + F) + (F + 9 * U)
+
+
+def run_padded(args, uh0, peak):
+    """The reference's default dealias rule (3/2 padding) on the headline
+    workload: fused padded passes, with the generic padded path beside it."""
+    import torch
+    n = args.n
+    out = {"workload": f"{n}^3 FP32 RK3 CFL 0.5, forcing as the headline, 3/2 padding "
+                       f"(transforms of {3 * n // 2} points)"}
+    for key, fused in (("fused", True), ("generic", False)):
+        sol = make_solver(n, dealias="3/2", fused=fused)
+        ss = sol.space_solver
+        ss.initialize_velocity(uh0, "fourier")
+        ss.step(2)
+        torch.cuda.synchronize()
+        k = args.padded_steps
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ss.step(k)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / k
+        out[f"{key}_ms_per_step"] = ms
+        out[f"{key}_value"] = n ** 3 / 1e6 / (ms / 1e3)
+        del ss, sol
+        torch.cuda.synchronize()
+    step_bytes = 3 * padded_stage_bytes(n)
+    out["unit"] = UNIT
+    out["alg_bytes_per_step"] = step_bytes
+    out["fused_frac_of_hbm"] = step_bytes / (out["fused_ms_per_step"] / 1e3) / 1e9 / peak
+    out["speedup_fused_vs_generic"] = out["generic_ms_per_step"] / out["fused_ms_per_step"]
     return out
 
 
@@ -450,6 +501,8 @@ def main():
     ap.add_argument("--ref-budget-s", type=float, default=120.0)
     ap.add_argument("--mode", choices=["headline", "ensemble", "serving"], default="headline")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-padded", action="store_true")
+    ap.add_argument("--padded-steps", type=int, default=10)
     ap.add_argument("--ens-steps", type=int, default=5000)
     ap.add_argument("--ens-scale", type=float, default=1.0)
     ap.add_argument("--ens-stepwise-sample", type=int, default=50)

@@ -116,6 +116,9 @@ struct FusedPlan {
   // measured best on B200 at 256^3 are P1 and P2 (16, 8) at >= 4 CTAs per
   // SM, P3 one staging buffer, 4 warps x 3 CTAs
   int var[6] = {0, 5, 5, 2, 0, 0};
+  // the same for 384-point passes (3/2 rule at n = 256), variants 11..16:
+  // P1, P2 twelve values and 8 columns at >= 2 CTAs per SM, P4 24 values
+  int var384[6] = {0, 11, 11, 0, 13, 0};
   // CTA rows per column tile of P1 (1 or 3) and P2 (1 or 2): one per group
   // of fields (PF_FUSED_SPLIT="p1:v,p2:v" overrides)
   int split[6] = {1, 3, 2, 1, 1, 1};
@@ -790,7 +793,10 @@ FusedPlan* fused_create(const Geo& g, int precision, int dealias) {
   if (const char* v = getenv("PF_FUSED_VARIANT")) {
     // "p1:1,p2:2,p4:1"
     for (const char* c = v; *c; ++c)
-      if (c[0] == 'p' && c[1] >= '1' && c[1] <= '5' && c[2] == ':') p->var[c[1] - '0'] = atoi(c + 3);
+      if (c[0] == 'p' && c[1] >= '1' && c[1] <= '5' && c[2] == ':') {
+        const int v = atoi(c + 3);
+        (v >= 11 ? p->var384 : p->var)[c[1] - '0'] = v;
+      }
   }
   if (const char* v = getenv("PF_FUSED_SPLIT")) {
     for (const char* c = v; *c; ++c)
@@ -897,6 +903,17 @@ static cudaError_t p4_run(FusedPlan* p, float2* nl, cudaStream_t st) {
 }
 
 #define PF_VARIANTS(RUN, N, ...)                                        \
+  if constexpr (N == 384) {                                             \
+    switch (var384) {                                                   \
+      case 11: return RUN<PAD, 384, 12, 8, 2>(__VA_ARGS__);             \
+      case 12: return RUN<PAD, 384, 12, 16, 1>(__VA_ARGS__);            \
+      case 13: return RUN<PAD, 384, 24, 8>(__VA_ARGS__);                \
+      case 14: return RUN<PAD, 384, 24, 8, 3>(__VA_ARGS__);             \
+      case 15: return RUN<PAD, 384, 24, 8, 4>(__VA_ARGS__);             \
+      case 16: return RUN<PAD, 384, 24, 16, 2>(__VA_ARGS__);            \
+      default: break;                                                   \
+    }                                                                   \
+  }                                                                     \
   if constexpr (N == 256) {                                             \
     switch (var) {                                                      \
       case 1: return RUN<PAD, 256, 8, 16>(__VA_ARGS__);                 \
@@ -911,15 +928,15 @@ static cudaError_t p4_run(FusedPlan* p, float2* nl, cudaStream_t st) {
   return RUN<PAD, N, TuneS<N>::E, TuneS<N>::T>(__VA_ARGS__);
 
 template <int N, bool PAD> static cudaError_t p1_n(FusedPlan* p, const float2* uh, cudaStream_t st) {
-  const int var = p->var[1];
+  const int var = p->var[1], var384 = p->var384[1];
   PF_VARIANTS(p1_run, N, p, uh, st)
 }
 template <int N, bool PAD> static cudaError_t p2_n(FusedPlan* p, cudaStream_t st) {
-  const int var = p->var[2];
+  const int var = p->var[2], var384 = p->var384[2];
   PF_VARIANTS(p2_run, N, p, st)
 }
 template <int N, bool PAD> static cudaError_t p4_n(FusedPlan* p, float2* nl, cudaStream_t st) {
-  const int var = p->var[4];
+  const int var = p->var[4], var384 = p->var384[4];
   PF_VARIANTS(p4_run, N, p, nl, st)
 }
 
