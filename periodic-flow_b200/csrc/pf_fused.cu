@@ -316,7 +316,7 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
   static_assert(NB == 1 || NB == 2, "one or two staging buffers per warp");
   static_assert(NB * W <= 16, "mbarriers fit the 128-byte header");
   using C = cx<R>;
-  extern __shared__ __align__(128) unsigned char smraw[];
+  extern __shared__ __align__(16) unsigned char smraw[];  // mbarriers 8 B, bulk copies 16 B
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int pw = lane / G, j = lane % G;
   const int fb = 2 * PW * f.c2;        // complex values of one field of a group
