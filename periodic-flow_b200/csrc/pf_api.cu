@@ -395,8 +395,7 @@ static int step_generic(pf_solver* h) {
     cudaError_t ue;
     if (use_fused) {
       tmark(h, PF_PASS_FUSED_P5);
-      if constexpr (sizeof(R) == 4) ue = fused_update(h->fused, A, h->ncomp, h->nl, h->st);
-      else ue = cudaErrorNotSupported;
+      ue = fused_update(h->fused, A, h->ncomp, h->nl, h->st);
       tmark(h, PF_PASS_FUSED_P5);
     } else {
       tmark(h, PF_PASS_UPDATE);
@@ -1015,9 +1014,10 @@ extern "C" int pf_footprint(const pf_config* c, unsigned long long* bytes) {
     }
   } else if (c->is_nonlinear) {
     b += cb * d * nspec + rsz * d * nphys + rsz * (d == 3 ? 3 : 1) * nphys;
-    bool pow2 = d == 3 && c->precision == PF_FP32 && c->fused && c->n[2] <= 256;
+    bool pow2 = d == 3 && c->fused && c->n[2] <= 256;
+    const int nmax = c->precision == PF_FP32 ? 512 : 256;
     for (int a = 0; pow2 && a < 3; ++a)
-      pow2 = c->n[a] >= 16 && c->n[a] <= 512 && (c->n[a] & (c->n[a] - 1)) == 0;
+      pow2 = c->n[a] >= 16 && c->n[a] <= nmax && (c->n[a] & (c->n[a] - 1)) == 0;
     if (pow2) {
       const unsigned long long k1 = (c->n[1] - 1) / 3, k2 = (c->n[2] - 1) / 3;
       b += cb * (5ull * c->n[0] * (2 * k1 + 1) * (k2 + 1) + 6ull * c->n[0] * c->n[1] * (k2 + 1));

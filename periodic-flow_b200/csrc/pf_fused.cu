@@ -29,19 +29,23 @@ namespace pf {
 
 // Transform lengths are 2^b (2/3 rule) or 3 * 2^b (3/2 rule, M = 3n/2); a
 // radix-3 first stage needs E divisible by 3.
-template <int N> struct TuneS {  // strided passes P1, P2, P4 (T measured best at 128 / G)
-  static constexpr int E = N % 3 == 0 ? 12 : (N <= 16 ? N : (N <= 64 ? 8 : 16));
+// FP64 (R = double) halves the values per lane of the FP32 choices (a complex
+// double takes four registers).
+template <int N, typename R = float> struct TuneS {  // strided passes P1, P2, P4 (T measured best at 128 / G)
+  static constexpr bool D = sizeof(R) == 8;
+  static constexpr int E = N % 3 == 0 ? 12
+                           : (D ? (N <= 8 ? N : 8) : (N <= 16 ? N : (N <= 64 ? 8 : 16)));
   static constexpr int G = N / E;
   static constexpr int T = (128 / G) < 8 ? 8 : ((128 / G) > 64 ? 64 : 128 / G);
 };
-template <int N> struct TuneU {  // P5 (FFT + update, three fields staged in smem)
-  static constexpr int E = TuneS<N>::E;
+template <int N, typename R = float> struct TuneU {  // P5 (FFT + update, three fields staged in smem)
+  static constexpr int E = TuneS<N, R>::E;
   static constexpr int G = N / E;
   static constexpr int T0 = (256 / G) < 4 ? 4 : ((256 / G) > 64 ? 64 : 256 / G);
-  // 3 * 2^b: the staging tile (3 N T values) kept near 100 KB
-  static constexpr int T = (N % 3 == 0 && 24 * N * T0 > 100 * 1024) ? T0 / 2 : T0;
+  // the staging tile (3 N T values) kept near 100 KB
+  static constexpr int T = 3 * N * T0 * (int)sizeof(cx<R>) > 100 * 1024 ? T0 / 2 : T0;
 };
-template <int N> struct TuneC {  // contiguous pass P3: 8 (2^b) or 12 (3 * 2^b) values per lane
+template <int N, typename R = float> struct TuneC {  // contiguous pass P3: 8 (2^b) or 12 (3 * 2^b) values per lane
   static constexpr int E = N % 3 == 0 ? 12 : 8;
   static constexpr int G = N / E;   // lanes per line pair, <= 32 for N <= 256 / 384
   static constexpr int PW = 32 / G; // line pairs per warp
@@ -50,9 +54,12 @@ template <int N> struct TuneC {  // contiguous pass P3: 8 (2^b) or 12 (3 * 2^b) 
   // p ^ ((p >> 3) & 15), which spreads the radix-8 stage stores (stride 8)
   // over all banks; the pair stride shifts neighbouring pairs' banks.  The
   // sides up to 16 and 3 * 2^b use a plain +1 per 16 padding instead.
-  static constexpr bool PLAIN = N <= 16 || N % 3 == 0;
-  static constexpr int BUF = PLAIN ? N + (N >> 4) + 1 : (N == 32 ? N + 4 : (N == 64 ? N + 8 : N));
-  static PF_HD int sw(int p) { return PLAIN ? p + (p >> 4) : p ^ ((p >> 3) & 15); }
+  static constexpr bool PLAIN = N <= 16 || N % 3 == 0 || sizeof(R) == 8;
+  static constexpr int SHP = sizeof(R) == 8 ? 3 : 4;  // FP64: +1 per 8 (16-byte values)
+  static constexpr int BUF = PLAIN ? N + (N >> SHP) + 1 : (N == 32 ? N + 4 : (N == 64 ? N + 8 : N));
+  static PF_HD int sw(int p) { return PLAIN ? p + (p >> SHP) : p ^ ((p >> 3) & 15); }
+  // FP64 P3 runs the streamed-omega kernel: 6 warps fit its shared memory
+  static constexpr int WS = sizeof(R) == 8 ? 6 : 8;
 };
 
 // Exchange buffer of the strided passes: position p of column t.  Eight
@@ -60,8 +67,8 @@ template <int N> struct TuneC {  // contiguous pass P3: 8 (2^b) or 12 (3 * 2^b) 
 // neighbouring threadIdx.y rows (positions 16 apart) on different banks when
 // T = 8.
 template <int T> PF_HD int col_pos(int p, int t) { return p * T + t + 8 * (p >> 4); }
-template <int N, int T> constexpr size_t col_buf_bytes() {
-  return sizeof(float2) * (size_t)(N * T + 8 * (N >> 4));
+template <int N, int T, typename R = float> constexpr size_t col_buf_bytes() {
+  return sizeof(cx<R>) * (size_t)(N * T + 8 * (N >> 4));
 }
 
 struct FGeo {
@@ -448,21 +455,23 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
   }
 }
 
-// P3 of the 3/2 rule: padded lines of t2 = 3 n2 / 2 points, inputs k2 <= n2/2
-// (the Nyquist column halved), outputs k2 <= n2/2 (the Nyquist entry plus its
-// -n2/2 partner, the conjugate).  Twelve values per lane and six fields would
-// not fit the registers, so u goes to thread-private shared-memory slots
-// after its C2R and omega is transformed one field at a time, accumulating
-// u x omega in registers.  One staging buffer per warp, refilled once the
-// group's last field is in registers.
-template <typename R, int N, int W>
+// P3 with omega streamed: u goes to thread-private shared-memory slots after
+// its C2R and omega is transformed one field at a time, accumulating u x
+// omega in registers, for when six whole fields would not fit the registers
+// (twelve values per lane on 3/2-rule lines, or FP64).  One staging buffer
+// per warp, refilled once the group's last field is in registers.
+// PAD (3/2 rule): padded lines of t2 = 3 n2 / 2 points, inputs k2 <= n2/2
+// (the Nyquist column halved), outputs k2 <= n2/2 (the Nyquist entry plus
+// its -n2/2 partner, the conjugate).  2/3 rule: inputs k2 <= kmax2, every
+// output k2 <= n2/2.
+template <typename R, int N, int W, bool PAD>
 __global__ void __launch_bounds__(32 * W, 1)
-k_p3pad(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
+k_p3s(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
         const cx<R>* __restrict__ tw, unsigned long long* __restrict__ maxbits, R scale,
         int* __restrict__ err, long long ngroups) {
-  constexpr int E = TuneC<N>::E, G = TuneC<N>::G, PW = TuneC<N>::PW;
+  constexpr int E = TuneC<N, R>::E, G = TuneC<N, R>::G, PW = TuneC<N, R>::PW;
   constexpr int H = N / 2;
-  constexpr int BUF = TuneC<N>::BUF;
+  constexpr int BUF = TuneC<N, R>::BUF;
   static_assert(G <= 32 && 32 % G == 0, "line pairs tile a warp");
   static_assert(W <= 16, "mbarriers fit the 128-byte header");
   using C = cx<R>;
@@ -492,7 +501,7 @@ k_p3pad(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
       for (int fld = 0; fld < 6; ++fld) bulk_g2s(wbase + fld * fb, src + fld * fs_in, fbytes, bar);
     }
   };
-  auto smf = [&](int pos) -> C& { return ex[TuneC<N>::sw(pos)]; };
+  auto smf = [&](int pos) -> C& { return ex[TuneC<N, R>::sw(pos)]; };
   auto sync = [] { __syncwarp(); };
   auto unpack = [&](const C* pa, C (&z)[E]) {
     const C* pb = pa + f.c2;
@@ -503,7 +512,7 @@ k_p3pad(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
       const bool kin = k < f.c2;
       C a = kin ? pa[k] : czero<C>();
       C b = kin ? pb[k] : czero<C>();
-      if (k == f.c2 - 1) { a = cscale(a, R(0.5)); b = cscale(b, R(0.5)); }
+      if (PAD && k == f.c2 - 1) { a = cscale(a, R(0.5)); b = cscale(b, R(0.5)); }
       if (m == 0) { a.y = 0; b.y = 0; }
       C r;
       if (m <= H) { r.x = a.x - b.y; r.y = a.y + b.x; }
@@ -586,7 +595,7 @@ k_p3pad(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
           C Av, Bv;
           Av.x = (zk.x + zn.x) * h; Av.y = (zk.y - zn.y) * h;
           Bv.x = (zk.y + zn.y) * h; Bv.y = -(zk.x - zn.x) * h;
-          if (k == f.nh - 1) {
+          if (PAD && k == f.nh - 1) {
             Av.x *= R(2); Av.y = R(0);
             Bv.x *= R(2); Bv.y = R(0);
           }
@@ -661,9 +670,9 @@ k_p4(cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
 // phase holds only a chunk of modes in registers; u_hat / u0 of a chunk are
 // loaded before any of its stores.
 template <typename R, int N, int NC, bool NOISE, int CHU, bool PAD>
-__global__ void __launch_bounds__(TuneU<N>::T * TuneU<N>::G, 2)
+__global__ void __launch_bounds__(TuneU<N, R>::T * TuneU<N, R>::G, sizeof(R) == 8 ? 1 : 2)
 k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
-  constexpr int E = TuneU<N>::E, G = TuneU<N>::G, T = TuneU<N>::T;
+  constexpr int E = TuneU<N, R>::E, G = TuneU<N, R>::G, T = TuneU<N, R>::T;
   constexpr int CH = E < CHU ? E : CHU;  // rows per thread whose state loads are in flight
   using C = cx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -760,12 +769,14 @@ template <typename K> static cudaError_t set_smem(K kern, size_t bytes) {
 static bool pow2(int n) { return n >= 16 && (n & (n - 1)) == 0; }
 
 FusedPlan* fused_create(const Geo& g, int precision, int dealias) {
-  if (g.dim != 3 || precision != 0 || (dealias != 0 && dealias != 1)) return nullptr;
+  if (g.dim != 3 || (precision != 0 && precision != 1) || (dealias != 0 && dealias != 1))
+    return nullptr;
   const bool pad = dealias == 1;
-  // 2/3 rule: sides 16..512 (the last up to 256); 3/2 rule: sides 16..256
-  // (transform lengths 24..384)
+  if (precision == 1 && pad) return nullptr;
+  // FP32 2/3 rule: sides 16..512 (the last up to 256); FP32 3/2 rule and
+  // FP64 2/3 rule: sides 16..256 (3/2 transform lengths 24..384)
   for (int a = 0; a < 3; ++a)
-    if (!pow2(g.n[a]) || g.n[a] > (pad ? 256 : 512)) return nullptr;
+    if (!pow2(g.n[a]) || g.n[a] > ((pad || precision == 1) ? 256 : 512)) return nullptr;
   if (g.n[2] > 256) return nullptr;
   FusedPlan* p = new FusedPlan();
   p->g = g;
@@ -853,113 +864,121 @@ void fused_destroy(FusedPlan* p) {
   }
 
 // Launch variants (radix width E, columns per CTA T, minimum CTAs per SM MB
-// that caps registers; 0: no cap) of the strided passes; variant 0 is the
-// TuneS default, 1..6 exist for n = 256 (tuning knob
+// that caps registers; 0: no cap) of the FP32 strided passes; variant 0 is
+// the TuneS default, 1..6 exist for n = 256 and 11..16 for 384 (tuning knob
 // PF_FUSED_VARIANT="p1:v,p2:v,p3:v,p4:v", which overrides FusedPlan::var).
-// The 3/2 rule always needs the exchange buffer (P4 folds through it).
-template <int N, int E, int T, int MB, bool PAD>
+// FP64 uses the TuneS defaults.  The 3/2 rule always needs the exchange
+// buffer (P4 folds through it).
+template <typename R, int N, int E, int T, bool PAD>
 constexpr size_t strided_smem() {
-  return (PAD || Plan<N, E>::stages() > 1) ? col_buf_bytes<N, T>() : 0;
+  return (PAD || Plan<N, E>::stages() > 1) ? col_buf_bytes<N, T, R>() : 0;
 }
 
-template <bool PAD, int N, int E, int T, int MB = 0>
-static cudaError_t p1_run(FusedPlan* p, const float2* uh, cudaStream_t st) {
+template <typename R, bool PAD, int N, int E, int T, int MB = 0>
+static cudaError_t p1_run(FusedPlan* p, const cx<R>* uh, cudaStream_t st) {
   constexpr int G = N / E;
-  const float2* tw = tw_base<float>() + tw_offset(N);
+  const cx<R>* tw = tw_base<R>() + tw_offset(N);
   const long long ncols = (long long)p->f.c1 * p->f.c2;
-  const size_t sm = strided_smem<N, E, T, MB, PAD>();
-  cudaError_t e = set_smem(k_p1<float, N, E, T, MB, PAD>, sm);
+  const size_t sm = strided_smem<R, N, E, T, PAD>();
+  cudaError_t e = set_smem(k_p1<R, N, E, T, MB, PAD>, sm);
   if (e != cudaSuccess) return e;
   const dim3 grid((unsigned)((ncols + T - 1) / T), (unsigned)p->split[1]);
-  k_p1<float, N, E, T, MB, PAD><<<grid, dim3(T, G), sm, st>>>(uh, (float2*)p->A, p->f, tw);
+  k_p1<R, N, E, T, MB, PAD><<<grid, dim3(T, G), sm, st>>>(uh, (cx<R>*)p->A, p->f, tw);
   return launched();
 }
 
-template <bool PAD, int N, int E, int T, int MB = 0>
+template <typename R, bool PAD, int N, int E, int T, int MB = 0>
 static cudaError_t p2_run(FusedPlan* p, cudaStream_t st) {
   constexpr int G = N / E;
-  const float2* tw = tw_base<float>() + tw_offset(N);
+  const cx<R>* tw = tw_base<R>() + tw_offset(N);
   const long long ncols = (long long)p->f.t0 * p->f.c2;
-  const size_t sm = strided_smem<N, E, T, MB, PAD>();
-  cudaError_t e = set_smem(k_p2<float, N, E, T, MB, PAD>, sm);
+  const size_t sm = strided_smem<R, N, E, T, PAD>();
+  cudaError_t e = set_smem(k_p2<R, N, E, T, MB, PAD>, sm);
   if (e != cudaSuccess) return e;
   const dim3 grid((unsigned)((ncols + T - 1) / T), (unsigned)p->split[2]);
-  k_p2<float, N, E, T, MB, PAD><<<grid, dim3(T, G), sm, st>>>(
-      (const float2*)p->A, (float2*)p->B, p->f, tw);
+  k_p2<R, N, E, T, MB, PAD><<<grid, dim3(T, G), sm, st>>>(
+      (const cx<R>*)p->A, (cx<R>*)p->B, p->f, tw);
   return launched();
 }
 
-template <bool PAD, int N, int E, int T, int MB = 0>
-static cudaError_t p4_run(FusedPlan* p, float2* nl, cudaStream_t st) {
+template <typename R, bool PAD, int N, int E, int T, int MB = 0>
+static cudaError_t p4_run(FusedPlan* p, cx<R>* nl, cudaStream_t st) {
   constexpr int G = N / E;
-  const float2* tw = tw_base<float>() + tw_offset(N);
+  const cx<R>* tw = tw_base<R>() + tw_offset(N);
   const long long ncols = (long long)3 * p->f.t0 * p->f.nh;
-  const size_t sm = strided_smem<N, E, T, MB, PAD>();
-  cudaError_t e = set_smem(k_p4<float, N, E, T, MB, PAD>, sm);
+  const size_t sm = strided_smem<R, N, E, T, PAD>();
+  cudaError_t e = set_smem(k_p4<R, N, E, T, MB, PAD>, sm);
   if (e != cudaSuccess) return e;
-  k_p4<float, N, E, T, MB, PAD><<<(unsigned)((ncols + T - 1) / T), dim3(T, G), sm, st>>>(
+  k_p4<R, N, E, T, MB, PAD><<<(unsigned)((ncols + T - 1) / T), dim3(T, G), sm, st>>>(
       nl, p->f, tw);
   return launched();
 }
 
 #define PF_VARIANTS(RUN, N, ...)                                        \
-  if constexpr (N == 384) {                                             \
+  if constexpr (sizeof(R) == 4 && N == 384) {                           \
     switch (var384) {                                                   \
-      case 11: return RUN<PAD, 384, 12, 8, 2>(__VA_ARGS__);             \
-      case 12: return RUN<PAD, 384, 12, 16, 1>(__VA_ARGS__);            \
-      case 13: return RUN<PAD, 384, 24, 8>(__VA_ARGS__);                \
-      case 14: return RUN<PAD, 384, 24, 8, 3>(__VA_ARGS__);             \
-      case 15: return RUN<PAD, 384, 24, 8, 4>(__VA_ARGS__);             \
-      case 16: return RUN<PAD, 384, 24, 16, 2>(__VA_ARGS__);            \
+      case 11: return RUN<R, PAD, 384, 12, 8, 2>(__VA_ARGS__);          \
+      case 12: return RUN<R, PAD, 384, 12, 16, 1>(__VA_ARGS__);         \
+      case 13: return RUN<R, PAD, 384, 24, 8>(__VA_ARGS__);             \
+      case 14: return RUN<R, PAD, 384, 24, 8, 3>(__VA_ARGS__);          \
+      case 15: return RUN<R, PAD, 384, 24, 8, 4>(__VA_ARGS__);          \
+      case 16: return RUN<R, PAD, 384, 24, 16, 2>(__VA_ARGS__);         \
       default: break;                                                   \
     }                                                                   \
   }                                                                     \
-  if constexpr (N == 256) {                                             \
+  if constexpr (sizeof(R) == 4 && N == 256) {                           \
     switch (var) {                                                      \
-      case 1: return RUN<PAD, 256, 8, 16>(__VA_ARGS__);                 \
-      case 2: return RUN<PAD, 256, 8, 32>(__VA_ARGS__);                 \
-      case 3: return RUN<PAD, 256, 16, 8>(__VA_ARGS__);                 \
-      case 4: return RUN<PAD, 256, 16, 8, 3>(__VA_ARGS__);              \
-      case 5: return RUN<PAD, 256, 16, 8, 4>(__VA_ARGS__);              \
-      case 6: return RUN<PAD, 256, 16, 16, 2>(__VA_ARGS__);             \
+      case 1: return RUN<R, PAD, 256, 8, 16>(__VA_ARGS__);              \
+      case 2: return RUN<R, PAD, 256, 8, 32>(__VA_ARGS__);              \
+      case 3: return RUN<R, PAD, 256, 16, 8>(__VA_ARGS__);              \
+      case 4: return RUN<R, PAD, 256, 16, 8, 3>(__VA_ARGS__);           \
+      case 5: return RUN<R, PAD, 256, 16, 8, 4>(__VA_ARGS__);           \
+      case 6: return RUN<R, PAD, 256, 16, 16, 2>(__VA_ARGS__);          \
       default: break;                                                   \
     }                                                                   \
   }                                                                     \
-  return RUN<PAD, N, TuneS<N>::E, TuneS<N>::T>(__VA_ARGS__);
+  return RUN<R, PAD, N, TuneS<N, R>::E, TuneS<N, R>::T>(__VA_ARGS__);
 
-template <int N, bool PAD> static cudaError_t p1_n(FusedPlan* p, const float2* uh, cudaStream_t st) {
+template <typename R, int N, bool PAD>
+static cudaError_t p1_n(FusedPlan* p, const cx<R>* uh, cudaStream_t st) {
   const int var = p->var[1], var384 = p->var384[1];
+  (void)var; (void)var384;
   PF_VARIANTS(p1_run, N, p, uh, st)
 }
-template <int N, bool PAD> static cudaError_t p2_n(FusedPlan* p, cudaStream_t st) {
+template <typename R, int N, bool PAD> static cudaError_t p2_n(FusedPlan* p, cudaStream_t st) {
   const int var = p->var[2], var384 = p->var384[2];
+  (void)var; (void)var384;
   PF_VARIANTS(p2_run, N, p, st)
 }
-template <int N, bool PAD> static cudaError_t p4_n(FusedPlan* p, float2* nl, cudaStream_t st) {
+template <typename R, int N, bool PAD>
+static cudaError_t p4_n(FusedPlan* p, cx<R>* nl, cudaStream_t st) {
   const int var = p->var[4], var384 = p->var384[4];
+  (void)var; (void)var384;
   PF_VARIANTS(p4_run, N, p, nl, st)
 }
 
-template <int N, int W>
-static cudaError_t p3pad_run(FusedPlan* p, float2* nl, unsigned long long* maxbits,
-                             cudaStream_t st) {
-  using TN = TuneC<N>;
-  const float2* tw = tw_base<float>() + tw_offset(N);
+// P3 with omega streamed (3/2 rule; FP64)
+template <typename R, bool PAD, int N, int W>
+static cudaError_t p3s_run(FusedPlan* p, cx<R>* nl, unsigned long long* maxbits,
+                           cudaStream_t st) {
+  using TN = TuneC<N, R>;
+  const cx<R>* tw = tw_base<R>() + tw_offset(N);
   const long long ngroups = (long long)p->f.t0 * p->f.t1 / (2 * TN::PW);
   const int fb = 2 * TN::PW * p->f.c2;
   const int WC = ((6 * fb + TN::PW * TN::BUF + TN::PW * 3 * N) + 15) & ~15;
-  const size_t sm = 128 + sizeof(float2) * (size_t)W * WC;
-  cudaError_t e = set_smem(k_p3pad<float, N, W>, sm);
+  const size_t sm = 128 + sizeof(cx<R>) * (size_t)W * WC;
+  cudaError_t e = set_smem(k_p3s<R, N, W, PAD>, sm);
   if (e != cudaSuccess) return e;
-  const float scale = (float)(1.0 / ((double)p->f.t0 * p->f.t1 * p->f.t2));
+  const R scale = (R)(1.0 / ((double)p->f.t0 * p->f.t1 * p->f.t2));
   long long blocks = (ngroups + W - 1) / W;
   if (blocks > (long long)p->nsm) blocks = p->nsm;
-  k_p3pad<float, N, W><<<(unsigned)blocks, 32 * W, sm, st>>>(
-      (const float2*)p->B, nl, p->f, tw, maxbits, scale, p->err, ngroups);
+  k_p3s<R, N, W, PAD><<<(unsigned)blocks, 32 * W, sm, st>>>(
+      (const cx<R>*)p->B, nl, p->f, tw, maxbits, scale, p->err, ngroups);
   return launched();
 }
 
-template <bool PAD, int N, int NB, int W, int MB>
+// FP32 2/3 rule: six fields in registers
+template <int N, int NB, int W, int MB>
 static cudaError_t p3_run(FusedPlan* p, float2* nl, unsigned long long* maxbits, cudaStream_t st) {
   using TN = TuneC<N>;
   const float2* tw = tw_base<float>() + tw_offset(N);
@@ -977,120 +996,123 @@ static cudaError_t p3_run(FusedPlan* p, float2* nl, unsigned long long* maxbits,
   return launched();
 }
 
-// Variant 0: two staging buffers per warp, 8 warps, one CTA per SM; 1..3
-// (n2 = 256): one staging buffer refilled as soon as the group is in
-// registers, with 8 warps x 2 CTAs, 4 warps x 3 CTAs or 8 warps x 1 CTA.
-// 3/2 rule: k_p3pad, 8 warps.
-template <int N, bool PAD>
-static cudaError_t p3_n(FusedPlan* p, float2* nl, unsigned long long* maxbits, cudaStream_t st) {
-  if constexpr (PAD) {
-    if constexpr (N > 384) return cudaErrorInvalidValue;
-    else return p3pad_run<N, 8>(p, nl, maxbits, st);
+// FP32 2/3 rule, variant 0: two staging buffers per warp, 8 warps, one CTA
+// per SM; 1..3 (n2 = 256): one staging buffer refilled as soon as the group
+// is in registers, with 8 warps x 2 CTAs, 4 warps x 3 CTAs or 8 warps x 1
+// CTA.  3/2 rule and FP64: the streamed-omega kernel.
+template <typename R, int N, bool PAD>
+static cudaError_t p3_n(FusedPlan* p, cx<R>* nl, unsigned long long* maxbits, cudaStream_t st) {
+  if constexpr (PAD || sizeof(R) == 8) {
+    if constexpr (N > 384 || (!PAD && N > 256)) return cudaErrorInvalidValue;
+    else return p3s_run<R, PAD, N, TuneC<N, R>::WS>(p, nl, maxbits, st);
   } else if constexpr (N > 256) {
     return cudaErrorInvalidValue;
   } else {
     if constexpr (N == 256) {
       switch (p->var[3]) {
-        case 1: return p3_run<PAD, 256, 1, 8, 2>(p, nl, maxbits, st);
-        case 2: return p3_run<PAD, 256, 1, 4, 3>(p, nl, maxbits, st);
-        case 3: return p3_run<PAD, 256, 1, 8, 1>(p, nl, maxbits, st);
+        case 1: return p3_run<256, 1, 8, 2>(p, nl, maxbits, st);
+        case 2: return p3_run<256, 1, 4, 3>(p, nl, maxbits, st);
+        case 3: return p3_run<256, 1, 8, 1>(p, nl, maxbits, st);
         default: break;
       }
     }
-    return p3_run<PAD, N, 2, TuneC<N>::W, 1>(p, nl, maxbits, st);
+    return p3_run<N, 2, TuneC<N>::W, 1>(p, nl, maxbits, st);
   }
 }
 
-template <bool PAD, int N, int CH>
-static cudaError_t p5_run(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, const float2* nl,
+template <typename R, bool PAD, int N, int CH>
+static cudaError_t p5_run(FusedPlan* p, const UpdateArgs<R>& U, int ncomp, const cx<R>* nl,
                           cudaStream_t st) {
-  using TN = TuneU<N>;
-  const float2* tw = tw_base<float>() + tw_offset(N);
+  using TN = TuneU<N, R>;
+  const cx<R>* tw = tw_base<R>() + tw_offset(N);
   const long long ncols = (long long)p->f.n1 * p->f.nh;
-  const size_t sm = sizeof(float2) * 3 * N * TN::T;
+  const size_t sm = sizeof(cx<R>) * 3 * N * TN::T;
   const dim3 grid((unsigned)((ncols + TN::T - 1) / TN::T)), block(TN::T, TN::G);
   cudaError_t e;
   if (U.noise_src == kNoiseNone) {
-    e = set_smem(k_p5<float, N, 3, false, CH, PAD>, sm);
+    e = set_smem(k_p5<R, N, 3, false, CH, PAD>, sm);
     if (e != cudaSuccess) return e;
-    k_p5<float, N, 3, false, CH, PAD><<<grid, block, sm, st>>>(U, nl, p->f, tw);
+    k_p5<R, N, 3, false, CH, PAD><<<grid, block, sm, st>>>(U, nl, p->f, tw);
   } else if (ncomp == 9) {
-    e = set_smem(k_p5<float, N, 9, true, CH, PAD>, sm);
+    e = set_smem(k_p5<R, N, 9, true, CH, PAD>, sm);
     if (e != cudaSuccess) return e;
-    k_p5<float, N, 9, true, CH, PAD><<<grid, block, sm, st>>>(U, nl, p->f, tw);
+    k_p5<R, N, 9, true, CH, PAD><<<grid, block, sm, st>>>(U, nl, p->f, tw);
   } else {
-    e = set_smem(k_p5<float, N, 3, true, CH, PAD>, sm);
+    e = set_smem(k_p5<R, N, 3, true, CH, PAD>, sm);
     if (e != cudaSuccess) return e;
-    k_p5<float, N, 3, true, CH, PAD><<<grid, block, sm, st>>>(U, nl, p->f, tw);
+    k_p5<R, N, 3, true, CH, PAD><<<grid, block, sm, st>>>(U, nl, p->f, tw);
   }
   return launched();
 }
 
-// Variant 0 keeps the state loads of 4 rows per thread in flight; 1, 2
-// (n0 = 256) use 2 and 8.
-template <int N, bool PAD>
-static cudaError_t p5_n(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, const float2* nl,
+// Variant 0 keeps the state loads of 4 rows per thread in flight (FP64: 2);
+// 1, 2 (FP32, n0 = 256) use 2 and 8.
+template <typename R, int N, bool PAD>
+static cudaError_t p5_n(FusedPlan* p, const UpdateArgs<R>& U, int ncomp, const cx<R>* nl,
                         cudaStream_t st) {
-  if constexpr (N == 256) {
+  if constexpr (sizeof(R) == 4 && N == 256) {
     switch (p->var[5]) {
-      case 1: return p5_run<PAD, 256, 2>(p, U, ncomp, nl, st);
-      case 2: return p5_run<PAD, 256, 8>(p, U, ncomp, nl, st);
+      case 1: return p5_run<R, PAD, 256, 2>(p, U, ncomp, nl, st);
+      case 2: return p5_run<R, PAD, 256, 8>(p, U, ncomp, nl, st);
       default: break;
     }
   }
-  return p5_run<PAD, N, 4>(p, U, ncomp, nl, st);
+  return p5_run<R, PAD, N, sizeof(R) == 8 ? 2 : 4>(p, U, ncomp, nl, st);
 }
 
 // 2/3 rule: nl is the caller's buffer in the state layout; 3/2 rule: passes 3
 // and 4 work in the plan's padded-grid buffer, which pass 5 reads.
-cudaError_t fused_pass(FusedPlan* p, int pass, const void* uhat, void* nl,
-                       unsigned long long* maxbits, cudaStream_t st) {
-  if (!p || !tw_base<float>()) return cudaErrorNotReady;
-  float2* nlp = p->pad ? (float2*)p->nlM : (float2*)nl;
-  if (p->pad) {
-    switch (pass) {
-      case 1: {
-#define PF_CALL(NN) p1_n<NN, true>(p, (const float2*)uhat, st)
-        PF_SWITCH_M(p->f.t0, PF_CALL)
+template <typename R>
+static cudaError_t pass_t(FusedPlan* p, int pass, const void* uhat, void* nl,
+                          unsigned long long* maxbits, cudaStream_t st) {
+  using C = cx<R>;
+  C* nlp = p->pad ? (C*)p->nlM : (C*)nl;
+  if constexpr (sizeof(R) == 4) {
+    if (p->pad) {
+      switch (pass) {
+        case 1: {
+#define PF_CALL(NN) p1_n<R, NN, true>(p, (const C*)uhat, st)
+          PF_SWITCH_M(p->f.t0, PF_CALL)
 #undef PF_CALL
-      }
-      case 2: {
-#define PF_CALL(NN) p2_n<NN, true>(p, st)
-        PF_SWITCH_M(p->f.t1, PF_CALL)
+        }
+        case 2: {
+#define PF_CALL(NN) p2_n<R, NN, true>(p, st)
+          PF_SWITCH_M(p->f.t1, PF_CALL)
 #undef PF_CALL
-      }
-      case 3: {
-#define PF_CALL(NN) p3_n<NN, true>(p, nlp, maxbits, st)
-        PF_SWITCH_M(p->f.t2, PF_CALL)
+        }
+        case 3: {
+#define PF_CALL(NN) p3_n<R, NN, true>(p, nlp, maxbits, st)
+          PF_SWITCH_M(p->f.t2, PF_CALL)
 #undef PF_CALL
-      }
-      case 4: {
-#define PF_CALL(NN) p4_n<NN, true>(p, nlp, st)
-        PF_SWITCH_M(p->f.t1, PF_CALL)
+        }
+        case 4: {
+#define PF_CALL(NN) p4_n<R, NN, true>(p, nlp, st)
+          PF_SWITCH_M(p->f.t1, PF_CALL)
 #undef PF_CALL
+        }
+        default:
+          return cudaErrorInvalidValue;
       }
-      default:
-        return cudaErrorInvalidValue;
     }
   }
   switch (pass) {
     case 1: {
-#define PF_CALL(NN) p1_n<NN, false>(p, (const float2*)uhat, st)
+#define PF_CALL(NN) p1_n<R, NN, false>(p, (const C*)uhat, st)
       PF_SWITCH_S(p->f.n0, PF_CALL)
 #undef PF_CALL
     }
     case 2: {
-#define PF_CALL(NN) p2_n<NN, false>(p, st)
+#define PF_CALL(NN) p2_n<R, NN, false>(p, st)
       PF_SWITCH_S(p->f.n1, PF_CALL)
 #undef PF_CALL
     }
     case 3: {
-#define PF_CALL(NN) p3_n<NN, false>(p, nlp, maxbits, st)
+#define PF_CALL(NN) p3_n<R, NN, false>(p, nlp, maxbits, st)
       PF_SWITCH_S(p->f.n2, PF_CALL)
 #undef PF_CALL
     }
     case 4: {
-#define PF_CALL(NN) p4_n<NN, false>(p, nlp, st)
+#define PF_CALL(NN) p4_n<R, NN, false>(p, nlp, st)
       PF_SWITCH_S(p->f.n1, PF_CALL)
 #undef PF_CALL
     }
@@ -1099,15 +1121,34 @@ cudaError_t fused_pass(FusedPlan* p, int pass, const void* uhat, void* nl,
   }
 }
 
+cudaError_t fused_pass(FusedPlan* p, int pass, const void* uhat, void* nl,
+                       unsigned long long* maxbits, cudaStream_t st) {
+  if (!p) return cudaErrorNotReady;
+  if (p->prec == 0) {
+    if (!tw_base<float>()) return cudaErrorNotReady;
+    return pass_t<float>(p, pass, uhat, nl, maxbits, st);
+  }
+  if (!tw_base<double>()) return cudaErrorNotReady;
+  return pass_t<double>(p, pass, uhat, nl, maxbits, st);
+}
+
 cudaError_t fused_update(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, const void* nl,
                          cudaStream_t st) {
-  if (!p || !tw_base<float>()) return cudaErrorNotReady;
+  if (!p || p->prec != 0 || !tw_base<float>()) return cudaErrorNotReady;
   if (p->pad) {
-#define PF_CALL(NN) p5_n<NN, true>(p, U, ncomp, (const float2*)p->nlM, st)
+#define PF_CALL(NN) p5_n<float, NN, true>(p, U, ncomp, (const float2*)p->nlM, st)
     PF_SWITCH_M(p->f.t0, PF_CALL)
 #undef PF_CALL
   }
-#define PF_CALL(NN) p5_n<NN, false>(p, U, ncomp, (const float2*)nl, st)
+#define PF_CALL(NN) p5_n<float, NN, false>(p, U, ncomp, (const float2*)nl, st)
+  PF_SWITCH_S(p->f.n0, PF_CALL)
+#undef PF_CALL
+}
+
+cudaError_t fused_update(FusedPlan* p, const UpdateArgs<double>& U, int ncomp, const void* nl,
+                         cudaStream_t st) {
+  if (!p || p->prec != 1 || p->pad || !tw_base<double>()) return cudaErrorNotReady;
+#define PF_CALL(NN) p5_n<double, NN, false>(p, U, ncomp, (const double2*)nl, st)
   PF_SWITCH_S(p->f.n0, PF_CALL)
 #undef PF_CALL
 }

@@ -6,8 +6,9 @@ namespace pf {
 
 struct FusedPlan;
 
-// Returns nullptr when no fused schedule is built for this geometry
-// (3D, FP32, 2/3 rule, power-of-two sides 16..512 with n2 <= 256).
+// Returns nullptr when no fused schedule is built for this geometry (3D,
+// power-of-two sides: FP32 2/3 rule 16..512 with n2 <= 256; FP32 3/2 rule
+// and FP64 2/3 rule 16..256).
 FusedPlan* fused_create(const Geo& g, int precision, int dealias);
 void fused_destroy(FusedPlan* p);
 // Pass 1..4 of the nonlinear term of uhat (unprojected) into nl; pass 3
@@ -16,6 +17,8 @@ cudaError_t fused_pass(FusedPlan* p, int pass, const void* uhat, void* nl,
                        unsigned long long* maxbits, cudaStream_t st);
 // Pass 5: forward FFT along axis 0 of nl fused with the stage update.
 cudaError_t fused_update(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, const void* nl,
+                         cudaStream_t st);
+cudaError_t fused_update(FusedPlan* p, const UpdateArgs<double>& U, int ncomp, const void* nl,
                          cudaStream_t st);
 
 // Error word of bounded device waits (0: none; synchronous read).

@@ -286,3 +286,34 @@ def test_fused_state_replaced_between_calls_and_graph_replay():
         s_.space_solver.replay()
         st.synchronize()
     assert rel_l2(a.space_solver.u_hat, b.space_solver.u_hat) < 2e-6
+
+
+@pytest.mark.parametrize("N", [(16, 16, 16), (32, 64, 32), (64, 32, 128), (128, 64, 64)])
+@pytest.mark.parametrize("integ", ["rk3", "rk4", "implicit_pc"])
+def test_fused_fp64_vs_oracle(N, integ):
+    """FP64 fused passes (the reference's precision) vs the FP64 oracle."""
+    o = O.OracleSolver(N, 2e-3, time_integrator=integ, viscosity=2e-3)
+    uh0 = O.spectral_random_field(o.grid, 9)
+    o.initialize(uh0, "fourier")
+    s = solver(N, dt=2e-3, time_integrator=integ, viscosity=2e-3, precision="fp64", fused=True)
+    s.initialize(uh0, "fourier")
+    o.advance(2)
+    s.space_solver.step(2)
+    assert rel_l2(s.space_solver.u_hat, o.u_hat) < 1e-11
+
+
+def test_fused_fp64_forcing_cfl_noise_matches_generic():
+    N = (64, 64, 64)
+    kw = dict(dt=1e-3, time_integrator="rk3", viscosity=2e-3, precision="fp64",
+              forcing=(0.1, 2.5), cfl=0.5, noise_mag=1e-3, seed=3)
+    a = solver(N, fused=True, **kw)
+    b = solver(N, fused=False, **kw)
+    uh0 = O.spectral_random_field(O.Grid(N), 1)
+    a.initialize(uh0, "fourier")
+    b.initialize(uh0, "fourier")
+    a.space_solver.step(3)
+    b.space_solver.step(3)
+    ta, sa, da = a.space_solver.time()
+    tb, sb, db = b.space_solver.time()
+    assert sa == sb == 3 and abs(da - db) < 1e-12 * db
+    assert rel_l2(a.space_solver.u_hat, b.space_solver.u_hat) < 1e-12
