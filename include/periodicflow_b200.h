@@ -131,6 +131,18 @@ int pf_step(pf_solver* h, int nsteps);
 int pf_graph_capture(pf_solver* h, int nsteps);
 int pf_graph_replay(pf_solver* h);
 
+/* Autotuner (no reference counterpart; the reference has one CPU schedule):
+ * times every launch variant of the fused passes 1-4 (radix width, columns
+ * per CTA, register cap, staging depth) on this solver's buffers and keeps
+ * the fastest; later solvers of the same geometry (precision, dealias rule,
+ * sides) in this process start from the picks.  Leaves the state unchanged;
+ * synchronous; not inside a graph capture.  picks (12 ints, may be NULL):
+ * variants of passes 0..5 for 256-point axes, then for 384-point axes.
+ * A no-op for solvers without the fused schedule. */
+int pf_autotune(pf_solver* h, int* picks);
+/* Current launch variants (same 12-int layout as pf_autotune). */
+int pf_fused_variants(pf_solver* h, int* out);
+
 /* Time, step counter and current dt (synchronises the stream). */
 int pf_get_time(pf_solver* h, double* t, long long* step, double* dt);
 /* Set time / step counter (restart). */

@@ -980,6 +980,23 @@ extern "C" int pf_graph_replay(pf_solver* h) {
   return PF_OK;
 }
 
+extern "C" int pf_autotune(pf_solver* h, int* picks) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  if (h->capturing) return fail(h, PF_ERR_INVALID, "pf_autotune: not inside a graph capture");
+  if (!h->fused) {  // nothing to choose: the per-operator path has one schedule
+    if (picks) fused_variants(nullptr, picks);
+    return PF_OK;
+  }
+  PF_CUDA(h, fused_autotune(h->fused, h->uhat, h->nl, h->st, picks));
+  return PF_OK;
+}
+
+extern "C" int pf_fused_variants(pf_solver* h, int* out) {
+  if (!h || !out) return fail(h, PF_ERR_INVALID, "pf_fused_variants: null argument");
+  fused_variants(h->fused, out);
+  return PF_OK;
+}
+
 extern "C" int pf_footprint(const pf_config* c, unsigned long long* bytes) {
   if (!c || !bytes) return fail(nullptr, PF_ERR_INVALID, "pf_footprint: null argument");
   int rc = validate(c);

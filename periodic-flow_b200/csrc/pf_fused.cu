@@ -17,8 +17,13 @@
 //   P5  forward FFT along axis 0 of nl, then the stage update of every mode
 //       of the column (Leray, Nyquist mask, forcing, noise, L, integrator)
 //       writing u_hat: the nonlinear term never returns to HBM.
+#include <array>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
 
 #include "pf_fft.cuh"
 #include "pf_fused.h"
@@ -768,6 +773,15 @@ template <typename K> static cudaError_t set_smem(K kern, size_t bytes) {
 
 static bool pow2(int n) { return n >= 16 && (n & (n - 1)) == 0; }
 
+// Launch variants picked by fused_autotune, per geometry (precision, rule,
+// sides); a later plan of the same geometry starts from them.
+using TuneKey = std::tuple<int, int, int, int, int>;
+static std::mutex g_tune_mu;
+static std::map<TuneKey, std::array<int, 12>> g_tuned;
+static TuneKey tune_key(const FusedPlan* p) {
+  return TuneKey(p->prec, p->pad ? 1 : 0, p->f.n0, p->f.n1, p->f.n2);
+}
+
 FusedPlan* fused_create(const Geo& g, int precision, int dealias) {
   if (g.dim != 3 || (precision != 0 && precision != 1) || (dealias != 0 && dealias != 1))
     return nullptr;
@@ -801,6 +815,16 @@ FusedPlan* fused_create(const Geo& g, int precision, int dealias) {
   f.cflw1 = g.n[1] * g.kscale[1] / (2.0 * M_PI);
   f.cflw2 = g.n[2] * g.kscale[2] / (2.0 * M_PI);
   f.nspec = g.nspec;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(tune_key(p));
+    if (it != g_tuned.end()) {
+      for (int i = 0; i < 6; ++i) {
+        p->var[i] = it->second[i];
+        p->var384[i] = it->second[6 + i];
+      }
+    }
+  }
   if (const char* v = getenv("PF_FUSED_VARIANT")) {
     // "p1:1,p2:2,p4:1"
     for (const char* c = v; *c; ++c)
@@ -1151,6 +1175,87 @@ cudaError_t fused_update(FusedPlan* p, const UpdateArgs<double>& U, int ncomp, c
 #define PF_CALL(NN) p5_n<double, NN, false>(p, U, ncomp, (const double2*)nl, st)
   PF_SWITCH_S(p->f.n0, PF_CALL)
 #undef PF_CALL
+}
+
+// Candidate launch variants of pass `pass` for this plan (the first is the
+// current choice); empty when the pass has only one.
+static std::vector<int> candidates(const FusedPlan* p, int pass, bool& is384) {
+  std::vector<int> c;
+  is384 = false;
+  if (p->prec != 0) return c;
+  const FGeo& f = p->f;
+  if (pass == 3) {
+    if (!p->pad && f.n2 == 256) c = {0, 1, 2, 3};
+    return c;
+  }
+  const int len = pass == 1 ? f.t0 : f.t1;
+  if (len == 256) {
+    c = {0, 1, 2, 3, 4, 5, 6};
+  } else if (len == 384) {
+    is384 = true;
+    c = {0, 11, 12, 13, 14, 15, 16};
+  }
+  return c;
+}
+
+cudaError_t fused_autotune(FusedPlan* p, const void* uhat, void* nl, cudaStream_t st,
+                           int* picks) {
+  if (!p) return cudaErrorInvalidValue;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return cudaGetLastError();
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return cudaGetLastError();
+  }
+  cudaError_t err = cudaSuccess;
+  // passes in order, so each one's input holds the previous pass's output
+  for (int pass = 1; pass <= 4 && err == cudaSuccess; ++pass) {
+    bool is384;
+    const std::vector<int> cand = candidates(p, pass, is384);
+    int* slot = is384 ? &p->var384[pass] : &p->var[pass];
+    const int keep = *slot;
+    float best = 1e30f;
+    int pick = keep;
+    for (size_t i = 0; i < cand.size() && err == cudaSuccess; ++i) {
+      *slot = cand[i];
+      err = fused_pass(p, pass, uhat, nl, nullptr, st);  // warm-up, first use of the variant
+      if (err != cudaSuccess) break;
+      float ms = 0.f;
+      cudaEventRecord(e0, st);
+      for (int r = 0; r < 5 && err == cudaSuccess; ++r) err = fused_pass(p, pass, uhat, nl, nullptr, st);
+      cudaEventRecord(e1, st);
+      if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+      if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+      if (err == cudaSuccess && ms < best) {
+        best = ms;
+        pick = cand[i];
+      }
+    }
+    *slot = err == cudaSuccess ? pick : keep;
+    if (cand.empty()) fused_pass(p, pass, uhat, nl, nullptr, st);  // keep the chain's inputs valid
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (err != cudaSuccess) return err;
+  std::array<int, 12> a;
+  for (int i = 0; i < 6; ++i) {
+    a[i] = p->var[i];
+    a[6 + i] = p->var384[i];
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[tune_key(p)] = a;
+  }
+  if (picks)
+    for (int i = 0; i < 12; ++i) picks[i] = a[i];
+  return cudaSuccess;
+}
+
+void fused_variants(const FusedPlan* p, int* out) {
+  for (int i = 0; i < 6; ++i) {
+    out[i] = p ? p->var[i] : 0;
+    out[6 + i] = p ? p->var384[i] : 0;
+  }
 }
 
 int fused_device_error(FusedPlan* p) {

@@ -71,6 +71,8 @@ _SIGS = [
     ("pf_step", C.c_int, [C.c_void_p, C.c_int]),
     ("pf_graph_capture", C.c_int, [C.c_void_p, C.c_int]),
     ("pf_graph_replay", C.c_int, [C.c_void_p]),
+    ("pf_autotune", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    ("pf_fused_variants", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     ("pf_get_time", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                               C.POINTER(C.c_double)]),
     ("pf_set_time", C.c_int, [C.c_void_p, C.c_double, C.c_longlong]),

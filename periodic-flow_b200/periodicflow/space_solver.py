@@ -234,6 +234,19 @@ class SpaceSolver(FourierSpace):
     def replay(self):
         N.check(N.lib().pf_graph_replay(self._h), self._h, "graph replay")
 
+    def autotune(self) -> dict:
+        """Time the launch variants of the fused passes on this solver's
+        buffers and keep the fastest (later solvers of the same geometry in
+        this process start from them).  The state is unchanged."""
+        picks = (C.c_int * 12)()
+        N.check(N.lib().pf_autotune(self._h, picks), self._h, "autotune")
+        return {"axes_256": list(picks[:6]), "axes_384": list(picks[6:])}
+
+    def fused_variants(self) -> dict:
+        out = (C.c_int * 12)()
+        N.check(N.lib().pf_fused_variants(self._h, out), self._h, "fused variants")
+        return {"axes_256": list(out[:6]), "axes_384": list(out[6:])}
+
     def time(self):
         t, s, dt = C.c_double(), C.c_longlong(), C.c_double()
         N.check(N.lib().pf_get_time(self._h, C.byref(t), C.byref(s), C.byref(dt)), self._h, "time")

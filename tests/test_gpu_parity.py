@@ -317,3 +317,25 @@ def test_fused_fp64_forcing_cfl_noise_matches_generic():
     tb, sb, db = b.space_solver.time()
     assert sa == sb == 3 and abs(da - db) < 1e-12 * db
     assert rel_l2(a.space_solver.u_hat, b.space_solver.u_hat) < 1e-12
+
+
+def test_autotune_keeps_state_and_parity():
+    """The autotuner leaves the state unchanged, picks among the built
+    variants, and the tuned fused path still agrees with the generic one."""
+    N = (256, 256, 256)
+    kw = dict(dt=1e-3, time_integrator="rk3", viscosity=2e-3, precision="fp32", cfl=0.5)
+    uh0 = O.spectral_random_field(O.Grid(N), 4)
+    a = solver(N, fused=True, **kw)
+    a.initialize(uh0, "fourier")
+    before = a.space_solver.u_hat
+    picks = a.space_solver.autotune()
+    assert np.array_equal(a.space_solver.u_hat, before)
+    assert all(0 <= v <= 6 for v in picks["axes_256"][1:5])
+    assert a.space_solver.fused_variants() == picks
+    a.space_solver.step(1)
+    ua = a.space_solver.u_hat
+    del a
+    b = solver(N, fused=False, **kw)
+    b.initialize(uh0, "fourier")
+    b.space_solver.step(1)
+    assert rel_l2(ua, b.space_solver.u_hat) < 2e-6
