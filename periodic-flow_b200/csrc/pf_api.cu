@@ -1031,10 +1031,15 @@ extern "C" int pf_footprint(const pf_config* c, unsigned long long* bytes) {
     }
   } else if (c->is_nonlinear) {
     b += cb * d * nspec + rsz * d * nphys + rsz * (d == 3 ? 3 : 1) * nphys;
-    bool pow2 = d == 3 && c->fused && c->n[2] <= 256;
+    bool pow2 = d == 3 && c->fused;
     const int nmax = c->precision == PF_FP32 ? 512 : 256;
-    for (int a = 0; pow2 && a < 3; ++a)
-      pow2 = c->n[a] >= 16 && c->n[a] <= nmax && (c->n[a] & (c->n[a] - 1)) == 0;
+    for (int a = 0; pow2 && a < 3; ++a) {
+      const int n = c->n[a], m = n / 3;
+      const bool p2 = n >= 16 && n <= nmax && (n & (n - 1)) == 0 && (a < 2 || n <= 256);
+      const bool t2 = c->precision == PF_FP32 && n % 3 == 0 && n >= 48 && n <= 384 &&
+                      (m & (m - 1)) == 0;
+      pow2 = p2 || t2;
+    }
     if (pow2) {
       const unsigned long long k1 = (c->n[1] - 1) / 3, k2 = (c->n[2] - 1) / 3;
       b += cb * (5ull * c->n[0] * (2 * k1 + 1) * (k2 + 1) + 6ull * c->n[0] * c->n[1] * (k2 + 1));

@@ -772,6 +772,11 @@ template <typename K> static cudaError_t set_smem(K kern, size_t bytes) {
 }
 
 static bool pow2(int n) { return n >= 16 && (n & (n - 1)) == 0; }
+// 3 * 2^b with 48 <= n
+static bool three_pow2(int n) {
+  const int m = n / 3;
+  return n % 3 == 0 && n >= 48 && (m & (m - 1)) == 0;
+}
 
 // Launch variants picked by fused_autotune, per geometry (precision, rule,
 // sides); a later plan of the same geometry starts from them.
@@ -787,11 +792,16 @@ FusedPlan* fused_create(const Geo& g, int precision, int dealias) {
     return nullptr;
   const bool pad = dealias == 1;
   if (precision == 1 && pad) return nullptr;
-  // FP32 2/3 rule: sides 16..512 (the last up to 256); FP32 3/2 rule and
-  // FP64 2/3 rule: sides 16..256 (3/2 transform lengths 24..384)
-  for (int a = 0; a < 3; ++a)
-    if (!pow2(g.n[a]) || g.n[a] > ((pad || precision == 1) ? 256 : 512)) return nullptr;
-  if (g.n[2] > 256) return nullptr;
+  // FP32 2/3 rule: sides 2^b 16..512 (the last up to 256) and 3 * 2^b
+  // 48..384; FP32 3/2 rule and FP64 2/3 rule: sides 2^b 16..256 (3/2
+  // transform lengths 24..384)
+  const bool t32 = precision == 0 && !pad;
+  for (int a = 0; a < 3; ++a) {
+    const bool ok = (pow2(g.n[a]) && g.n[a] <= ((pad || precision == 1) ? 256 : 512)) ||
+                    (t32 && three_pow2(g.n[a]) && g.n[a] <= 384);
+    if (!ok) return nullptr;
+  }
+  if (g.n[2] > (t32 && three_pow2(g.n[2]) ? 384 : 256)) return nullptr;
   FusedPlan* p = new FusedPlan();
   p->g = g;
   p->prec = precision;
@@ -873,6 +883,21 @@ void fused_destroy(FusedPlan* p) {
     case 64: return CALL(64);     \
     case 128: return CALL(128);   \
     case 256: return CALL(256);   \
+    case 512: return CALL(512);   \
+    default: return cudaErrorInvalidValue; \
+  }
+// FP32 2/3-rule sides: powers of two and 3 * 2^b (48..384)
+#define PF_SWITCH_T(n, CALL)      \
+  switch (n) {                    \
+    case 16: return CALL(16);     \
+    case 32: return CALL(32);     \
+    case 48: return CALL(48);     \
+    case 64: return CALL(64);     \
+    case 96: return CALL(96);     \
+    case 128: return CALL(128);   \
+    case 192: return CALL(192);   \
+    case 256: return CALL(256);   \
+    case 384: return CALL(384);   \
     case 512: return CALL(512);   \
     default: return cudaErrorInvalidValue; \
   }
@@ -1023,11 +1048,11 @@ static cudaError_t p3_run(FusedPlan* p, float2* nl, unsigned long long* maxbits,
 // FP32 2/3 rule, variant 0: two staging buffers per warp, 8 warps, one CTA
 // per SM; 1..3 (n2 = 256): one staging buffer refilled as soon as the group
 // is in registers, with 8 warps x 2 CTAs, 4 warps x 3 CTAs or 8 warps x 1
-// CTA.  3/2 rule and FP64: the streamed-omega kernel.
+// CTA.  3/2 rule, FP64 and 3 * 2^b sides: the streamed-omega kernel.
 template <typename R, int N, bool PAD>
 static cudaError_t p3_n(FusedPlan* p, cx<R>* nl, unsigned long long* maxbits, cudaStream_t st) {
-  if constexpr (PAD || sizeof(R) == 8) {
-    if constexpr (N > 384 || (!PAD && N > 256)) return cudaErrorInvalidValue;
+  if constexpr (PAD || sizeof(R) == 8 || N % 3 == 0) {
+    if constexpr (N > 384 || (!PAD && N % 3 != 0 && N > 256)) return cudaErrorInvalidValue;
     else return p3s_run<R, PAD, N, TuneC<N, R>::WS>(p, nl, maxbits, st);
   } else if constexpr (N > 256) {
     return cudaErrorInvalidValue;
@@ -1119,6 +1144,32 @@ static cudaError_t pass_t(FusedPlan* p, int pass, const void* uhat, void* nl,
       }
     }
   }
+  if constexpr (sizeof(R) == 4) {
+    switch (pass) {
+      case 1: {
+#define PF_CALL(NN) p1_n<R, NN, false>(p, (const C*)uhat, st)
+        PF_SWITCH_T(p->f.n0, PF_CALL)
+#undef PF_CALL
+      }
+      case 2: {
+#define PF_CALL(NN) p2_n<R, NN, false>(p, st)
+        PF_SWITCH_T(p->f.n1, PF_CALL)
+#undef PF_CALL
+      }
+      case 3: {
+#define PF_CALL(NN) p3_n<R, NN, false>(p, nlp, maxbits, st)
+        PF_SWITCH_T(p->f.n2, PF_CALL)
+#undef PF_CALL
+      }
+      case 4: {
+#define PF_CALL(NN) p4_n<R, NN, false>(p, nlp, st)
+        PF_SWITCH_T(p->f.n1, PF_CALL)
+#undef PF_CALL
+      }
+      default:
+        return cudaErrorInvalidValue;
+    }
+  }
   switch (pass) {
     case 1: {
 #define PF_CALL(NN) p1_n<R, NN, false>(p, (const C*)uhat, st)
@@ -1165,7 +1216,7 @@ cudaError_t fused_update(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, co
 #undef PF_CALL
   }
 #define PF_CALL(NN) p5_n<float, NN, false>(p, U, ncomp, (const float2*)nl, st)
-  PF_SWITCH_S(p->f.n0, PF_CALL)
+  PF_SWITCH_T(p->f.n0, PF_CALL)
 #undef PF_CALL
 }
 

@@ -6,9 +6,9 @@ namespace pf {
 
 struct FusedPlan;
 
-// Returns nullptr when no fused schedule is built for this geometry (3D,
-// power-of-two sides: FP32 2/3 rule 16..512 with n2 <= 256; FP32 3/2 rule
-// and FP64 2/3 rule 16..256).
+// Returns nullptr when no fused schedule is built for this geometry (3D:
+// FP32 2/3 rule, sides 2^b 16..512 with n2 <= 256 and 3 * 2^b 48..384; FP32
+// 3/2 rule and FP64 2/3 rule, sides 2^b 16..256).
 FusedPlan* fused_create(const Geo& g, int precision, int dealias);
 void fused_destroy(FusedPlan* p);
 // Pass 1..4 of the nonlinear term of uhat (unprojected) into nl; pass 3
