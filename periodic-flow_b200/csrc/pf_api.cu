@@ -2,6 +2,7 @@
 // reference's time loop (simulation.py:205-217) on one CUDA stream.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -55,8 +56,21 @@ struct pf_solver {
   int graph_steps = 0;
   long long graph_launches = 0;
   bool capturing = false;
+  // private one-step graph of pf_step (noise-free, no history, no timer):
+  // recorded on its own stream, replayed once per step on st
+  cudaGraph_t agraph = nullptr;
+  cudaGraphExec_t agexec = nullptr;
+  cudaStream_t astream = nullptr;
+  long long a_launches = 0;
+  bool auto_graph = true;
   std::string err;
 };
+
+// Kernel arguments recorded in the private step graph change: record again.
+static void drop_auto_graph(pf_solver* h) {
+  if (h->agexec) { cudaGraphExecDestroy(h->agexec); h->agexec = nullptr; }
+  if (h->agraph) { cudaGraphDestroy(h->agraph); h->agraph = nullptr; }
+}
 
 // record an event on the solver stream when `pass` is the timed pass; events
 // come in (begin, end) pairs around each launch of that pass
@@ -460,6 +474,37 @@ static int flush_hist(pf_solver* h) {
   return PF_OK;
 }
 
+// Record one step (step_generic) as a graph on the private stream.
+template <typename R>
+static int record_auto_graph(pf_solver* h) {
+  if (!h->astream) PF_CUDA(h, cudaStreamCreateWithFlags(&h->astream, cudaStreamNonBlocking));
+  cudaStream_t user = h->st;
+  h->st = h->astream;
+  const long long l0 = launch_total();
+  h->capturing = true;
+  cudaError_t e = cudaStreamBeginCapture(h->astream, cudaStreamCaptureModeThreadLocal);
+  int rc = PF_OK;
+  if (e == cudaSuccess) {
+    rc = step_generic<R>(h);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(h->astream, &g);
+    if (e == cudaSuccess) e = e2;
+    h->agraph = g;
+  }
+  h->capturing = false;
+  h->st = user;
+  h->a_launches = launch_total() - l0;
+  add_launches(-h->a_launches);  // recorded, not launched
+  if (rc == PF_OK && e == cudaSuccess) e = cudaGraphInstantiate(&h->agexec, h->agraph, 0);
+  if (rc != PF_OK || e != cudaSuccess) {
+    drop_auto_graph(h);
+    cudaGetLastError();
+    h->auto_graph = false;  // step without it from now on
+    return rc != PF_OK ? rc : fail(h, PF_ERR_CUDA, std::string("step graph: ") + cudaGetErrorString(e));
+  }
+  return PF_OK;
+}
+
 template <typename R>
 static int step_impl(pf_solver* h, int nsteps) {
   const bool stokes_fast = !h->cfg.is_nonlinear && h->cfg.forcing_eps <= 0.0 &&
@@ -469,6 +514,23 @@ static int step_impl(pf_solver* h, int nsteps) {
     return fail(h, PF_ERR_INVALID,
                 "injected noise: call pf_inject_noise before every single pf_step(h, 1)");
   int done = 0;
+  // noise-free runs without history or timer: one recorded step graph per
+  // step (the step's launches cost one graph launch; dt, time and the CFL
+  // reduction live in device scalars, so the graph is step-independent)
+  const bool graphable = !stokes_fast && h->auto_graph && !injected && noise_src(h) == kNoiseNone &&
+                         !h->record_hist && h->tpass < 0 && nsteps >= 2;
+  if (graphable) {
+    if (!h->agexec) {
+      int rc = record_auto_graph<R>(h);
+      if (rc) return rc;
+    }
+    for (; done < nsteps; ++done) {
+      PF_CUDA(h, cudaGraphLaunch(h->agexec, h->st));
+      add_launches(h->a_launches);
+      h->step += 1;
+    }
+    return PF_OK;
+  }
   while (done < nsteps) {
     int chunk = nsteps - done;
     if (h->record_hist) chunk = 1;
@@ -631,6 +693,7 @@ int pf_create(const pf_config* cfg, pf_solver** out) {
   if (cfg->is_nonlinear && cfg->fused) {
     h->fused = fused_create(g, h->prec, cfg->dealias);  // nullptr when no fused path fits
   }
+  if (const char* v = getenv("PF_STEP_GRAPH")) h->auto_graph = atoi(v) != 0;  // 0: plain launches
   *out = h;
   return PF_OK;
 }
@@ -646,6 +709,8 @@ int pf_destroy(pf_solver* h) {
   for (cudaEvent_t e : h->tev) cudaEventDestroy(e);
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->graph) cudaGraphDestroy(h->graph);
+  drop_auto_graph(h);
+  if (h->astream) cudaStreamDestroy(h->astream);
   delete h;
   return PF_OK;
 }
@@ -792,11 +857,13 @@ static int set_scalar_field(pf_solver* h, void** slot, const double* src, int wh
 
 int pf_set_linear_operator(pf_solver* h, const double* L, int where) {
   if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  drop_auto_graph(h);  // the operator array may be newly allocated
   return set_scalar_field(h, &h->lop, L, where);
 }
 
 int pf_set_correlation(pf_solver* h, const double* C, int where) {
   if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  drop_auto_graph(h);
   return set_scalar_field(h, &h->corr, C, where);
 }
 
@@ -988,6 +1055,7 @@ extern "C" int pf_autotune(pf_solver* h, int* picks) {
     return PF_OK;
   }
   PF_CUDA(h, fused_autotune(h->fused, h->uhat, h->nl, h->st, picks));
+  drop_auto_graph(h);  // record the new launch variants
   return PF_OK;
 }
 

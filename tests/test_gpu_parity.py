@@ -369,3 +369,25 @@ def test_fused_192_matches_generic():
         out.append(s.space_solver.u_hat)
         del s
     assert rel_l2(out[0], out[1]) < 2e-6
+
+
+def test_step_graph_matches_plain_launches(monkeypatch):
+    """pf_step replays a recorded one-step graph for noise-free runs; the
+    states equal plain launches bit for bit, also after the linear operator
+    is set between calls (the graph is recorded again)."""
+    N = (32, 32, 32)
+    kw = dict(dt=2e-3, time_integrator="rk3", viscosity=2e-3, precision="fp32",
+              forcing=(0.1, 2.5), cfl=0.5)
+    uh0 = O.spectral_random_field(O.Grid(N), 8)
+    a = solver(N, **kw)
+    monkeypatch.setenv("PF_STEP_GRAPH", "0")
+    b = solver(N, **kw)
+    monkeypatch.delenv("PF_STEP_GRAPH")
+    L = -2e-3 * O.Grid(N).k2 * 1.5
+    for s_ in (a, b):
+        s_.initialize(uh0, "fourier")
+        s_.space_solver.step(4)
+        s_.set_linear_operator(L)
+        s_.space_solver.step(3)
+    assert np.array_equal(a.space_solver.u_hat, b.space_solver.u_hat)
+    assert a.space_solver.time() == b.space_solver.time()
