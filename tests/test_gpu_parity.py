@@ -391,3 +391,25 @@ def test_step_graph_matches_plain_launches(monkeypatch):
         s_.space_solver.step(3)
     assert np.array_equal(a.space_solver.u_hat, b.space_solver.u_hat)
     assert a.space_solver.time() == b.space_solver.time()
+
+
+def test_tgv64_fp64_full_run_vs_reference_history():
+    """The Taylor-Green configuration for its full 400 steps (64^3 FP64,
+    rk4, dt 0.005, nu 1/1600, 2/3 rule) through the solver's public API,
+    against the energy/enstrophy history and final low modes produced by the
+    reference's own kernels (tests/golden/make_c1_history.py)."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "tgv64_fp64_rk4_400.npz"))
+    ref = z["energy_enstrophy"]
+    n = 64
+    s = solver((n, n, n), dt=0.005, time_integrator="rk4", viscosity=1 / 1600,
+               precision="fp64", diagnostics=True)
+    g = O.Grid((n, n, n))
+    s.initialize(O.taylor_green(g))
+    s.space_solver.step(400)
+    hs = s.space_solver.history()
+    assert hs.shape == ref.shape
+    assert np.max(np.abs(hs - ref) / np.abs(ref)) < 1e-10
+    idx = np.r_[0:4, n - 3:n]
+    low = s.space_solver.u_hat[:, idx][:, :, idx][..., 0:4]
+    assert rel_l2(low, z["final_low_modes"]) < 1e-9

@@ -116,3 +116,17 @@ def test_tgv_energy_decay_rate():
     e1 = O.energy(s.grid, s.u_hat)
     rate = (e1 - e0) / 1e-4
     assert abs(rate - (-2 * nu * z0)) < 1e-6
+
+
+def test_oracle_tgv64_history_prefix():
+    """The oracle's Taylor-Green run (64^3 FP64, rk4, dt 0.005, nu 1/1600)
+    against the energy/enstrophy history the reference's kernels produced
+    (tests/golden/make_c1_history.py); first 40 of its 400 steps."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "tgv64_fp64_rk4_400.npz"))
+    ref = z["energy_enstrophy"]
+    n = 64
+    o = O.OracleSolver((n, n, n), 0.005, time_integrator="rk4", viscosity=1 / 1600)
+    o.initialize(O.taylor_green(o.grid))
+    h = np.array(o.advance(40, diagnostics=True))
+    np.testing.assert_allclose(h, ref[:40], rtol=1e-12, atol=0)
