@@ -525,18 +525,34 @@ def run_ensemble(args):
 
 
 def run_serving(args):
+    """The serving configuration (continuous batching vs one request at a
+    time through the public API), and a mix of small requests only, where a
+    single solve leaves most of the GPU idle.  serial_in_service is the sum of
+    the serial requests' service times (set-up included) over the serial
+    makespan."""
     from periodicflow.serving import Server, poisson_requests
+
+    def one(reqs, label):
+        srv = Server(hbm_budget=150e9)
+        cont = srv.run(reqs, "continuous")
+        ser = srv.run(reqs, "serial")
+        busy = sum(r.finished - r.admitted for r in reqs) / ser["makespan_s"]  # serial run's times
+        return {"workload": label, "continuous": cont, "serial": ser,
+                "serial_in_service": busy,
+                "throughput_ratio": cont["mpts_steps_per_s"] / ser["mpts_steps_per_s"],
+                "p50_ratio": ser["p50_latency_s"] / cont["p50_latency_s"],
+                "p99_ratio": ser["p99_latency_s"] / cont["p99_latency_s"]}
+
     reqs = poisson_requests(args.serve_requests, rate=50.0, seed=2,
                             max_steps=args.serve_max_steps)
-    srv = Server(hbm_budget=150e9)
-    cont = srv.run(reqs, "continuous")
-    ser = srv.run(reqs, "serial")
-    return {"workload": f"{len(reqs)} Poisson requests (50/s, seed 2): 2D 64^2-1024^2 and 3D "
-                        f"32^3-128^3 log-uniform, Taylor-Green or thermal noise, "
-                        f"100-{args.serve_max_steps} steps, 150 GB budget",
-            "continuous": cont, "serial": ser,
-            "throughput_ratio": cont["mpts_steps_per_s"] / ser["mpts_steps_per_s"],
-            "p99_ratio": ser["p99_latency_s"] / cont["p99_latency_s"]}
+    out = one(reqs, f"{len(reqs)} Poisson requests (50/s, seed 2): 2D 64^2-1024^2 and 3D "
+                    f"32^3-128^3 log-uniform, Taylor-Green or thermal noise, "
+                    f"100-{args.serve_max_steps} steps, 150 GB budget")
+    small = poisson_requests(120, rate=200.0, seed=3, min_steps=100, max_steps=2000,
+                             sizes2d=(64, 128, 256), sizes3d=(16, 32, 64))
+    out["small_requests"] = one(small, "120 Poisson requests (200/s, seed 3): 2D 64^2-256^2 and "
+                                       "3D 16^3-64^3, Taylor-Green or thermal noise, 100-2000 steps")
+    return out
 
 
 def cpu_baseline(n, steps):

@@ -169,68 +169,117 @@ class Server:
         return self._metrics(reqs, "serial")
 
     def _run_continuous(self, reqs, torch):
+        """Event-driven continuous batching: every nonlinear request advances
+        on its own stream by graph-replayed chunks and gets its next chunk as
+        soon as its previous one has completed (polled with CUDA events), so
+        small requests are not held back by large ones; all linear requests
+        advance together as one captured ensemble graph on a stream of its
+        own, re-captured at a chunk boundary when its membership changes.
+        Arrivals are admitted against the memory budget and slot limit as
+        they come."""
         from .ensemble import Ensemble
         t0 = time.perf_counter()
         pending = list(reqs)
-        active = []        # (request, solver, remaining, footprint, stream)
+        nl = []            # [request, solver, remaining, footprint, stream, event]
+        lin = []           # [request, solver, remaining, footprint]
+        lin_wait = []      # admitted linear requests waiting for the next chunk boundary
+        ens = None
+        ens_chunk = 0
+        ens_event = None
+        ens_stream = torch.cuda.Stream()
         used = 0
-        ens, ens_ids = None, ()
-        while pending or active:
-            now = time.perf_counter() - t0
-            while (pending and pending[0].arrival <= now and len(active) < self.max_slots):
+
+        def admit(now):
+            nonlocal used
+            while pending and pending[0].arrival <= now and \
+                    len(nl) + len(lin) + len(lin_wait) < self.max_slots:
                 r = pending[0]
                 fp = self.footprint(r)
-                if used + fp > self.budget and active:
+                if used + fp > self.budget and (nl or lin or lin_wait):
                     break  # wait for memory to free up
                 pending.pop(0)
                 r.admitted = time.perf_counter() - t0
                 sol = make_solver(r, self.precision)
-                stream = None
-                if not r.linear:
-                    # own stream; a chunk of steps captured once as a CUDA graph
-                    stream = torch.cuda.Stream()
-                    sol.space_solver.set_stream(stream)
-                    if r.steps >= self.chunk_nl:
-                        sol.space_solver.capture(self.chunk_nl)
-                active.append([r, sol, r.steps, fp, stream])
                 used += fp
-            if not active:
-                if pending:
-                    time.sleep(max(0.0, pending[0].arrival - (time.perf_counter() - t0)))
-                continue
-            torch.cuda.synchronize()  # set-up copies of new members are done
-            # nonlinear requests: a chunk each on its own stream (asynchronous)
-            for a in active:
-                if not a[0].linear:
-                    c = min(self.chunk_nl, a[2])
-                    if c == self.chunk_nl:
-                        a[1].space_solver.replay()
-                    else:
-                        a[1].space_solver.step(c)
-                    a[2] -= c
-            # linear requests: one ensemble launch for all of them
-            lin = [a for a in active if a[0].linear]
-            if lin:
-                ids = tuple(a[0].rid for a in lin)
-                if ids != ens_ids:
-                    ens = Ensemble([a[1] for a in lin])
-                    ens_ids = ids
-                c = min(self.chunk_lin, min(a[2] for a in lin))
-                ens.step(c)
-                for a in lin:
-                    a[2] -= c
-            torch.cuda.synchronize()
+                if r.linear:
+                    lin_wait.append([r, sol, r.steps, fp])
+                    continue
+                stream = torch.cuda.Stream()
+                sol.space_solver.set_stream(stream)
+                torch.cuda.current_stream().synchronize()  # set-up copies done
+                if r.steps >= self.chunk_nl:
+                    sol.space_solver.capture(self.chunk_nl)
+                a = [r, sol, r.steps, fp, stream, torch.cuda.Event()]
+                launch_nl(a)
+                nl.append(a)
+
+        def launch_nl(a):
+            c = min(self.chunk_nl, a[2])
+            if c == self.chunk_nl:
+                a[1].space_solver.replay()
+            else:
+                a[1].space_solver.step(c)
+            a[2] -= c
+            a[5].record(a[4])
+
+        def relaunch_linear():
+            nonlocal ens, ens_chunk, ens_event
+            lin.extend(lin_wait)
+            lin_wait.clear()
+            if not lin:
+                ens = None
+                return
+            torch.cuda.current_stream().synchronize()
+            ens_chunk = min(self.chunk_lin, min(a[2] for a in lin))
+            ens = Ensemble([a[1] for a in lin])
+            ens.capture(ens_chunk, ens_stream)
+            ens.replay()
+            ens_event = torch.cuda.Event()
+            ens_event.record(ens_stream)
+
+        while pending or nl or lin or lin_wait:
+            admit(time.perf_counter() - t0)
+            progressed = False
             keep = []
-            for a in active:
+            for a in nl:
+                if not a[5].query():
+                    keep.append(a)
+                    continue
+                progressed = True
                 if a[2] == 0:
                     self._finish(a[0], a[1], t0)
                     used -= a[3]
                 else:
+                    launch_nl(a)
                     keep.append(a)
-            if len(keep) != len(active):
-                if any(a[0].linear for a in active if a not in keep):
-                    ens, ens_ids = None, ()
-                active = keep
+            nl[:] = keep
+            if ens is None:
+                if lin_wait:
+                    relaunch_linear()
+                    progressed = True
+            elif ens_event.query():
+                progressed = True
+                for a in lin:
+                    a[2] -= ens_chunk
+                done = [a for a in lin if a[2] == 0]
+                for a in done:
+                    self._finish(a[0], a[1], t0)
+                    used -= a[3]
+                left = [a for a in lin if a[2] > 0]
+                # a new chunk length (or membership) needs a new capture
+                if done or lin_wait or (left and min(a[2] for a in left) < ens_chunk):
+                    lin[:] = left
+                    ens = None
+                    relaunch_linear()
+                else:
+                    ens.replay()
+                    ens_event.record(ens_stream)
+            if not progressed:
+                if not (nl or lin or lin_wait) and pending:
+                    time.sleep(max(0.0, pending[0].arrival - (time.perf_counter() - t0)))
+                else:
+                    time.sleep(5e-5)
+        torch.cuda.synchronize()
         return self._metrics(reqs, "continuous")
 
     @staticmethod
