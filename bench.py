@@ -236,6 +236,9 @@ def run_ours(args, dist, rank, world):
     padded = None
     if rank == 0 and not args.no_padded and not pad:
         padded = run_padded(args, uh0, peak)
+    fp64 = None
+    if rank == 0 and not args.no_fp64 and not pad:
+        fp64 = run_fp64(args, uh0)
     cufft = None
     if rank == 0 and not args.no_cufft and not pad:
         cufft = run_cufft_comparison(args, uh0)
@@ -258,7 +261,7 @@ def run_ours(args, dist, rank, world):
             "gpu_launches": int(c1.value - c0.value),
             "clocks": ck, "roofline": roofline, "step_roofline": step_roof,
             "e2e": e2e, "cpu_baseline": cpu, "batched": ensemble, "padded_3_2": padded,
-            "cufft_comparison": cufft,
+            "cufft_comparison": cufft, "fp64": fp64,
         }
         print(json.dumps(line), flush=True)
 
@@ -436,6 +439,40 @@ def padded_stage_bytes(n):
     NL = 3 * t * t * nh * cb
     F = 3 * t * n * nh * cb
     return (3 * U + A) + (A + B) + (B + NL) + (NL + F) + (F + 9 * U)
+
+
+def run_fp64(args, uh0):
+    """The headline workload in FP64 (the reference's precision) through the
+    fused FP64 schedule, and the FP32 state's error against it after the same
+    steps from the same initial field (both runs step-by-step identical in
+    dt: the CFL step is taken in each precision)."""
+    import torch
+    n = args.n
+    k = args.fp64_steps
+    out = {"workload": f"{n}^3 headline workload in FP64 (fused FP64 schedule)"}
+    states = {}
+    for prec in ("fp64", "fp32"):
+        sol = make_solver(n, precision=prec)
+        ss = sol.space_solver
+        ss.initialize_velocity(uh0, "fourier")
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ss.step(k)
+        e1.record()
+        torch.cuda.synchronize()
+        if prec == "fp64":
+            ms = e0.elapsed_time(e1) / k
+            out["ms_per_step"] = ms
+            out["value"] = n ** 3 / 1e6 / (ms / 1e3)
+            out["unit"] = UNIT
+        states[prec] = ss.u_hat
+        del ss, sol
+        torch.cuda.synchronize()
+    a, b = states["fp32"], states["fp64"]
+    out["steps"] = k
+    out["fp32_rel_l2_vs_fp64"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    return out
 
 
 def run_padded(args, uh0, peak):
@@ -635,6 +672,8 @@ def main():
     ap.add_argument("--no-padded", action="store_true")
     ap.add_argument("--no-cufft", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--fp64-steps", type=int, default=10)
     ap.add_argument("--cufft-steps", type=int, default=20)
     ap.add_argument("--padded-steps", type=int, default=10)
     ap.add_argument("--ens-steps", type=int, default=5000)
