@@ -125,19 +125,21 @@ struct FusedPlan {
   int* err = nullptr; // device error word (bounded waits that gave up)
   int nsm = 148;
   // launch variant per pass (used where that pass's axis has 256 points):
-  // measured best on B200 at 256^3 are P1 and P2 (16, 8) at >= 4 CTAs per
-  // SM, P3 one staging buffer, 4 warps x 3 CTAs
-  int var[6] = {0, 5, 5, 2, 0, 0};
-  // the same for 384-point passes (3/2 rule at n = 256), variants 11..16:
-  // P1, P2 twelve values and 8 columns at >= 2 CTAs per SM, P4 24 values
-  int var384[6] = {0, 11, 11, 0, 13, 0};
+  // measured best on B200 at 256^3 are P1 one output field per CTA row
+  // (16, 8), P2 (16, 8) at >= 4 CTAs per SM, P3 one staging buffer, 4 warps
+  // x 3 CTAs
+  int var[6] = {0, 7, 5, 2, 0, 0};
+  // the same for 384-point passes (3/2 rule at n = 256), variants 11..19:
+  // P1 one output field per CTA row at 24 values, P2 the same at twelve
+  // values, P4 24 values
+  int var384[6] = {0, 17, 18, 0, 13, 0};
   // CTA rows per column tile of P1 (1 or 3) and P2 (1 or 2): one per group
   // of fields (PF_FUSED_SPLIT="p1:v,p2:v" overrides)
   int split[6] = {1, 3, 2, 1, 1, 1};
 };
 
 // ---------------------------------------------------------------------- P1
-template <typename R, int N, int E, int T, int MB, bool PAD>
+template <typename R, int N, int E, int T, int MB, bool PAD, bool FIVE = false>
 __global__ void __launch_bounds__(T * (N / E), MB)
 k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
      const cx<R>* __restrict__ tw) {
@@ -179,6 +181,25 @@ k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
   // gridDim.y == 3: block row y transforms field y alone (u0; u1 and D1;
   // u2 and D2), which triples the CTAs without extra traffic
   const int part = gridDim.y == 1 ? -1 : (int)blockIdx.y;
+  if constexpr (FIVE) {
+    // FIVE: block row y makes output field y alone (u0, u1, u2, D1, D2) with
+    // one line buffer; the derivative rows re-read u1, u2
+    const int fld = blockIdx.y;
+    const int c = fld < 3 ? fld : fld - 2;
+    C w[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      int kf;
+      w[e] = load(c, e, kf);
+      if (fld >= 3) w[e] = cmuli(cscale(w[e], (R)(f.ks0 * kf)));
+    }
+    fft<N, E, +1>(w, j, tw, smf, sync);
+    if (active) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) A[fld * fs_out + (j + G * e) * ncols + q] = w[e];
+    }
+    return;
+  }
   C v[E], w[E];
   if (part <= 0) {
 #pragma unroll
@@ -214,7 +235,7 @@ k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
 }
 
 // ---------------------------------------------------------------------- P2
-template <typename R, int N, int E, int T, int MB, bool PAD>
+template <typename R, int N, int E, int T, int MB, bool PAD, bool SIX = false>
 __global__ void __launch_bounds__(T * (N / E), MB)
 k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
      const cx<R>* __restrict__ tw) {
@@ -273,6 +294,43 @@ k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
   // gridDim.y == 2: block row 0 makes omega0, u1, u2 (reads u1, u2), row 1
   // omega2, omega1, u0 (reads u0, D1, D2); twice the CTAs, no extra traffic
   const int part = gridDim.y == 1 ? -1 : (int)blockIdx.y;
+  if constexpr (SIX) {
+    // SIX: block row y makes output field y' alone with one line buffer
+    // (omega fields read their two inputs): one FFT per CTA, fewer registers,
+    // at the cost of re-reading u0, u1, u2
+    C w[E];
+    switch (blockIdx.y) {
+      case 0:  // omega0 = i (k1 u2 - k2 u1)
+#pragma unroll
+        for (int e = 0; e < E; ++e) w[e] = cmuli(csub(cscale(ld(2, e), k1(e)), cscale(ld(1, e), k2)));
+        fft<N, E, +1>(w, j, tw, smf, sync);
+        store(3, w);
+        break;
+      case 1:
+      case 2:
+      case 5: {  // u1, u2, u0
+        const int fld = blockIdx.y == 5 ? 0 : (int)blockIdx.y;
+#pragma unroll
+        for (int e = 0; e < E; ++e) w[e] = ld(fld, e);
+        fft<N, E, +1>(w, j, tw, smf, sync);
+        store(fld, w);
+        break;
+      }
+      case 3:  // omega2 = D1 - i k1 u0
+#pragma unroll
+        for (int e = 0; e < E; ++e) w[e] = csub(ld(3, e), cmuli(cscale(ld(0, e), k1(e))));
+        fft<N, E, +1>(w, j, tw, smf, sync);
+        store(5, w);
+        break;
+      default:  // omega1 = i k2 u0 - D2
+#pragma unroll
+        for (int e = 0; e < E; ++e) w[e] = csub(cmuli(cscale(ld(0, e), k2)), ld(4, e));
+        fft<N, E, +1>(w, j, tw, smf, sync);
+        store(4, w);
+        break;
+    }
+    return;
+  }
   C a[E], b[E], w[E];
   if (part <= 0) {
     // omega0 = i (k1 u2 - k2 u1); u1; u2
@@ -914,7 +972,9 @@ void fused_destroy(FusedPlan* p) {
 
 // Launch variants (radix width E, columns per CTA T, minimum CTAs per SM MB
 // that caps registers; 0: no cap) of the FP32 strided passes; variant 0 is
-// the TuneS default, 1..6 exist for n = 256 and 11..16 for 384 (tuning knob
+// the TuneS default, 1..6 exist for n = 256 and 11..16 for 384, and P1 / P2
+// also have one-output-field-per-CTA-row forms (7, 8 at 256; 17..19 at 384)
+// (tuning knob
 // PF_FUSED_VARIANT="p1:v,p2:v,p3:v,p4:v", which overrides FusedPlan::var).
 // FP64 uses the TuneS defaults.  The 3/2 rule always needs the exchange
 // buffer (P4 folds through it).
@@ -988,15 +1048,72 @@ static cudaError_t p4_run(FusedPlan* p, cx<R>* nl, cudaStream_t st) {
   }                                                                     \
   return RUN<R, PAD, N, TuneS<N, R>::E, TuneS<N, R>::T>(__VA_ARGS__);
 
+// P1 with one output field per CTA row (five rows)
+template <typename R, bool PAD, int N, int E, int T, int MB = 0>
+static cudaError_t p1five_run(FusedPlan* p, const cx<R>* uh, cudaStream_t st) {
+  constexpr int G = N / E;
+  const cx<R>* tw = tw_base<R>() + tw_offset(N);
+  const long long ncols = (long long)p->f.c1 * p->f.c2;
+  const size_t sm = strided_smem<R, N, E, T, PAD>();
+  cudaError_t e = set_smem(k_p1<R, N, E, T, MB, PAD, true>, sm);
+  if (e != cudaSuccess) return e;
+  const dim3 grid((unsigned)((ncols + T - 1) / T), 5);
+  k_p1<R, N, E, T, MB, PAD, true><<<grid, dim3(T, G), sm, st>>>(uh, (cx<R>*)p->A, p->f, tw);
+  return launched();
+}
+
 template <typename R, int N, bool PAD>
 static cudaError_t p1_n(FusedPlan* p, const cx<R>* uh, cudaStream_t st) {
   const int var = p->var[1], var384 = p->var384[1];
   (void)var; (void)var384;
+  if constexpr (sizeof(R) == 4 && N == 384) {
+    switch (var384) {
+      case 17: return p1five_run<R, PAD, 384, 24, 8>(p, uh, st);
+      case 18: return p1five_run<R, PAD, 384, 12, 8>(p, uh, st);
+      default: break;
+    }
+  }
+  if constexpr (sizeof(R) == 4 && N == 256) {
+    switch (var) {
+      case 7: return p1five_run<R, PAD, 256, 16, 8>(p, uh, st);
+      default: break;
+    }
+  }
   PF_VARIANTS(p1_run, N, p, uh, st)
 }
+// P2 with one output field per CTA row (six rows)
+template <typename R, bool PAD, int N, int E, int T, int MB = 0>
+static cudaError_t p2six_run(FusedPlan* p, cudaStream_t st) {
+  constexpr int G = N / E;
+  const cx<R>* tw = tw_base<R>() + tw_offset(N);
+  const long long ncols = (long long)p->f.t0 * p->f.c2;
+  const size_t sm = strided_smem<R, N, E, T, PAD>();
+  cudaError_t e = set_smem(k_p2<R, N, E, T, MB, PAD, true>, sm);
+  if (e != cudaSuccess) return e;
+  const dim3 grid((unsigned)((ncols + T - 1) / T), 6);
+  k_p2<R, N, E, T, MB, PAD, true><<<grid, dim3(T, G), sm, st>>>(
+      (const cx<R>*)p->A, (cx<R>*)p->B, p->f, tw);
+  return launched();
+}
+
 template <typename R, int N, bool PAD> static cudaError_t p2_n(FusedPlan* p, cudaStream_t st) {
   const int var = p->var[2], var384 = p->var384[2];
   (void)var; (void)var384;
+  if constexpr (sizeof(R) == 4 && N == 384) {
+    switch (var384) {
+      case 17: return p2six_run<R, PAD, 384, 24, 8>(p, st);
+      case 18: return p2six_run<R, PAD, 384, 12, 8>(p, st);
+      case 19: return p2six_run<R, PAD, 384, 24, 16>(p, st);
+      default: break;
+    }
+  }
+  if constexpr (sizeof(R) == 4 && N == 256) {
+    switch (var) {
+      case 7: return p2six_run<R, PAD, 256, 16, 8>(p, st);
+      case 8: return p2six_run<R, PAD, 256, 16, 8, 4>(p, st);
+      default: break;
+    }
+  }
   PF_VARIANTS(p2_run, N, p, st)
 }
 template <typename R, int N, bool PAD>
@@ -1242,9 +1359,13 @@ static std::vector<int> candidates(const FusedPlan* p, int pass, bool& is384) {
   const int len = pass == 1 ? f.t0 : f.t1;
   if (len == 256) {
     c = {0, 1, 2, 3, 4, 5, 6};
+    if (pass == 2) c.insert(c.end(), {7, 8});
+    if (pass == 1) c.push_back(7);
   } else if (len == 384) {
     is384 = true;
     c = {0, 11, 12, 13, 14, 15, 16};
+    if (pass == 2) c.insert(c.end(), {17, 18, 19});
+    if (pass == 1) c.insert(c.end(), {17, 18});
   }
   return c;
 }
