@@ -1112,6 +1112,10 @@ extern "C" int pf_footprint(const pf_config* c, unsigned long long* bytes) {
       const unsigned long long k1 = (c->n[1] - 1) / 3, k2 = (c->n[2] - 1) / 3;
       b += cb * (5ull * c->n[0] * (2 * k1 + 1) * (k2 + 1) + 6ull * c->n[0] * c->n[1] * (k2 + 1));
     }
+    bool f2 = d == 2 && c->fused;
+    for (int a = 0; f2 && a < 2; ++a)
+      f2 = c->n[a] >= 16 && c->n[a] <= 1024 && (c->n[a] & (c->n[a] - 1)) == 0;
+    if (f2) b += cb * 3ull * c->n[0] * ((c->n[1] - 1) / 3 + 1);  // 2D fused pass-1 scratch
   }
   if (c->noise_mag != 0.0 && c->noise_source == PF_NOISE_SRC_INJECTED) b += cb * 2 * ncomp * nspec;
   *bytes = b;

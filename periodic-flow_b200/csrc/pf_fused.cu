@@ -27,6 +27,7 @@
 
 #include "pf_fft.cuh"
 #include "pf_fused.h"
+#include "pf_fused2d.h"
 #include "pf_tma.cuh"
 #include "pf_update.cuh"
 
@@ -116,12 +117,14 @@ PF_D int fold_src(int i, int t, int n) {
 
 struct FusedPlan {
   Geo g;
-  FGeo f;
+  FGeo f{};
   int prec;
   void* A = nullptr;  // 5 * t0 * c1 * c2 complex
   void* B = nullptr;  // 6 * t0 * t1 * c2 complex
   void* nlM = nullptr;  // 3/2 rule: 3 * t0 * t1 * nh complex (nl on the padded x0, x1 grid)
   bool pad = false;
+  int dim = 3;        // 2: the three-pass 2D schedule of pf_fused2d.cu on f2 (A its scratch)
+  F2 f2;
   int* err = nullptr; // device error word (bounded waits that gave up)
   int nsm = 148;
   // launch variant per pass (used where that pass's axis has 256 points):
@@ -848,9 +851,29 @@ static TuneKey tune_key(const FusedPlan* p) {
   return TuneKey(p->prec, p->pad ? 1 : 0, p->f.n0, p->f.n1, p->f.n2);
 }
 
-FusedPlan* fused_create(const Geo& g, int precision, int dealias) {
-  if (g.dim != 3 || (precision != 0 && precision != 1) || (dealias != 0 && dealias != 1))
+static FusedPlan* fused_create_2d(const Geo& g, int precision) {
+  if (!fused2d_side(g.n[0]) || !fused2d_side(g.n[1])) return nullptr;
+  FusedPlan* p = new FusedPlan();
+  p->g = g;
+  p->prec = precision;
+  p->dim = 2;
+  p->f2 = fused2d_geo(g);
+  const size_t cb = precision == 0 ? 8 : 16;
+  if (cudaMalloc(&p->A, cb * fused2d_scratch_elems(p->f2)) != cudaSuccess ||
+      cudaMalloc(&p->err, sizeof(int)) != cudaSuccess ||
+      cudaMemset(p->err, 0, sizeof(int)) != cudaSuccess) {
+    fused_destroy(p);
+    cudaGetLastError();
     return nullptr;
+  }
+  return p;
+}
+
+FusedPlan* fused_create(const Geo& g, int precision, int dealias) {
+  if ((precision != 0 && precision != 1) || (dealias != 0 && dealias != 1)) return nullptr;
+  // 2D: 2/3 rule, sides 2^b 16..1024, FP32 and FP64
+  if (g.dim == 2) return dealias == 0 ? fused_create_2d(g, precision) : nullptr;
+  if (g.dim != 3) return nullptr;
   const bool pad = dealias == 1;
   if (precision == 1 && pad) return nullptr;
   // FP32 2/3 rule: sides 2^b 16..512 (the last up to 256) and 3 * 2^b
@@ -1323,9 +1346,26 @@ static cudaError_t pass_t(FusedPlan* p, int pass, const void* uhat, void* nl,
   }
 }
 
+// 2D plans: pass 1 is Q1, pass 3 is Q2 (into the caller's nl), 2 and 4 have
+// nothing to do.
+template <typename R>
+static cudaError_t pass_2d(FusedPlan* p, int pass, const void* uhat, void* nl,
+                           unsigned long long* maxbits, cudaStream_t st) {
+  switch (pass) {
+    case 1: return fused2d_inverse<R>(p->f2, (const cx<R>*)uhat, (cx<R>*)p->A, st);
+    case 3: return fused2d_products<R>(p->f2, (const cx<R>*)p->A, (cx<R>*)nl, maxbits, st);
+    case 2:
+    case 4: return cudaSuccess;
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 cudaError_t fused_pass(FusedPlan* p, int pass, const void* uhat, void* nl,
                        unsigned long long* maxbits, cudaStream_t st) {
   if (!p) return cudaErrorNotReady;
+  if (p->dim == 2)
+    return p->prec == 0 ? pass_2d<float>(p, pass, uhat, nl, maxbits, st)
+                        : pass_2d<double>(p, pass, uhat, nl, maxbits, st);
   if (p->prec == 0) {
     if (!tw_base<float>()) return cudaErrorNotReady;
     return pass_t<float>(p, pass, uhat, nl, maxbits, st);
@@ -1337,6 +1377,7 @@ cudaError_t fused_pass(FusedPlan* p, int pass, const void* uhat, void* nl,
 cudaError_t fused_update(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, const void* nl,
                          cudaStream_t st) {
   if (!p || p->prec != 0 || !tw_base<float>()) return cudaErrorNotReady;
+  if (p->dim == 2) return fused2d_update<float>(p->f2, U, ncomp, (const float2*)nl, st);
   if (p->pad) {
 #define PF_CALL(NN) p5_n<float, NN, true>(p, U, ncomp, (const float2*)p->nlM, st)
     PF_SWITCH_M(p->f.t0, PF_CALL)
@@ -1350,6 +1391,7 @@ cudaError_t fused_update(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, co
 cudaError_t fused_update(FusedPlan* p, const UpdateArgs<double>& U, int ncomp, const void* nl,
                          cudaStream_t st) {
   if (!p || p->prec != 1 || p->pad || !tw_base<double>()) return cudaErrorNotReady;
+  if (p->dim == 2) return fused2d_update<double>(p->f2, U, ncomp, (const double2*)nl, st);
 #define PF_CALL(NN) p5_n<double, NN, false>(p, U, ncomp, (const double2*)nl, st)
   PF_SWITCH_S(p->f.n0, PF_CALL)
 #undef PF_CALL
@@ -1360,7 +1402,7 @@ cudaError_t fused_update(FusedPlan* p, const UpdateArgs<double>& U, int ncomp, c
 static std::vector<int> candidates(const FusedPlan* p, int pass, bool& is384) {
   std::vector<int> c;
   is384 = false;
-  if (p->prec != 0) return c;
+  if (p->prec != 0 || p->dim != 3) return c;
   const FGeo& f = p->f;
   if (pass == 3) {
     if (!p->pad && f.n2 == 256) c = {0, 1, 2, 3};
@@ -1383,6 +1425,10 @@ static std::vector<int> candidates(const FusedPlan* p, int pass, bool& is384) {
 cudaError_t fused_autotune(FusedPlan* p, const void* uhat, void* nl, cudaStream_t st,
                            int* picks) {
   if (!p) return cudaErrorInvalidValue;
+  if (p->dim != 3) {  // the 2D schedule has one launch form per pass
+    if (picks) fused_variants(p, picks);
+    return cudaSuccess;
+  }
   cudaEvent_t e0, e1;
   if (cudaEventCreate(&e0) != cudaSuccess) return cudaGetLastError();
   if (cudaEventCreate(&e1) != cudaSuccess) {

@@ -1,4 +1,5 @@
-// Fused pencil passes of the 3D nonlinear term (u x omega with the 2/3 rule).
+// Fused pencil passes of the nonlinear term (u x omega): 3D five-pass
+// schedule, 2D three-pass schedule (pf_fused2d.cu).
 #pragma once
 #include "pf_kernels.h"
 
@@ -8,7 +9,9 @@ struct FusedPlan;
 
 // Returns nullptr when no fused schedule is built for this geometry (3D:
 // FP32 2/3 rule, sides 2^b 16..512 with n2 <= 256 and 3 * 2^b 48..384; FP32
-// 3/2 rule and FP64 2/3 rule, sides 2^b 16..256).
+// 3/2 rule and FP64 2/3 rule, sides 2^b 16..256; 2D: 2/3 rule, FP32 and
+// FP64, sides 2^b 16..1024).  2D plans run passes 1 and 3 and the update;
+// passes 2 and 4 are no-ops there.
 FusedPlan* fused_create(const Geo& g, int precision, int dealias);
 void fused_destroy(FusedPlan* p);
 // Pass 1..4 of the nonlinear term of uhat (unprojected) into nl; pass 3
