@@ -303,8 +303,9 @@ def run_e2e(args, uh0, rank, dist, dealias="2/3"):
     state_b = int(np.prod(uh0.shape)) * 16
     return {"value": world * n ** 3 / 1e6 * K / sec, "unit": UNIT, "steps": K,
             "h2d_bytes_per_step": state_b / K, "d2h_bytes_per_step": (state_b + 16 * K) / K,
-            "note": "per step: pf_step(1) + E,Z read-back (16 B); state up/download "
-                    "(complex128) amortised over the steps; wall clock"}
+            "note": "one whole run of the configuration's length: state upload (complex128), "
+                    "then per step pf_step(1) + E,Z read-back (16 B), then state download; "
+                    "wall clock"}
 
 
 def ensemble_members(scale=1.0, precision="fp32"):
@@ -660,7 +661,8 @@ def main():
     ap.add_argument("--traffic", type=float, default=None,
                     help="DRAM bytes per launch of the timed pass from an ncu capture")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=50)
+    # the forced-turbulence configuration's full run: 2000 steps, E and Z every step
+    ap.add_argument("--e2e-steps", type=int, default=2000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--ref-budget-s", type=float, default=120.0)

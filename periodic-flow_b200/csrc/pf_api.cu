@@ -1089,7 +1089,7 @@ extern "C" int pf_footprint(const pf_config* c, unsigned long long* bytes) {
       mph *= m;
     }
     b += cb * d * nspec + cb * 3 * msp + rsz * d * mph + rsz * (d == 3 ? 3 : 1) * mph;
-    bool fz = d == 3 && c->precision == PF_FP32 && c->fused && c->n[2] <= 256;
+    bool fz = d == 3 && c->fused && c->n[2] <= 256;
     for (int a = 0; fz && a < 3; ++a)
       fz = c->n[a] >= 16 && c->n[a] <= 256 && (c->n[a] & (c->n[a] - 1)) == 0;
     if (fz) {  // fused 3/2 schedule: pass buffers on the padded x0 (and x1) grid

@@ -875,10 +875,9 @@ FusedPlan* fused_create(const Geo& g, int precision, int dealias) {
   if (g.dim == 2) return dealias == 0 ? fused_create_2d(g, precision) : nullptr;
   if (g.dim != 3) return nullptr;
   const bool pad = dealias == 1;
-  if (precision == 1 && pad) return nullptr;
   // FP32 2/3 rule: sides 2^b 16..512 (the last up to 256) and 3 * 2^b
-  // 48..384; FP32 3/2 rule and FP64 2/3 rule: sides 2^b 16..256 (3/2
-  // transform lengths 24..384)
+  // 48..384; 3/2 rule (FP32, FP64) and FP64 2/3 rule: sides 2^b 16..256
+  // (3/2 transform lengths 24..384)
   const bool t32 = precision == 0 && !pad;
   for (int a = 0; a < 3; ++a) {
     const bool ok = (pow2(g.n[a]) && g.n[a] <= ((pad || precision == 1) ? 256 : 512)) ||
@@ -1106,7 +1105,7 @@ static cudaError_t p1_n(FusedPlan* p, const cx<R>* uh, cudaStream_t st) {
       default: break;
     }
   }
-  if constexpr (sizeof(R) == 8 && !PAD && N >= 64) {
+  if constexpr (sizeof(R) == 8 && N >= 48) {
     if (p->fp64_rows) return p1five_run<R, PAD, N, TuneS<N, R>::E, TuneS<N, R>::T>(p, uh, st);
   }
   PF_VARIANTS(p1_run, N, p, uh, st)
@@ -1144,7 +1143,7 @@ template <typename R, int N, bool PAD> static cudaError_t p2_n(FusedPlan* p, cud
       default: break;
     }
   }
-  if constexpr (sizeof(R) == 8 && !PAD && N >= 64) {
+  if constexpr (sizeof(R) == 8 && N >= 48) {
     if (p->fp64_rows) return p2six_run<R, PAD, N, TuneS<N, R>::E, TuneS<N, R>::T>(p, st);
   }
   PF_VARIANTS(p2_run, N, p, st)
@@ -1203,6 +1202,8 @@ template <typename R, int N, bool PAD>
 static cudaError_t p3_n(FusedPlan* p, cx<R>* nl, unsigned long long* maxbits, cudaStream_t st) {
   if constexpr (PAD || sizeof(R) == 8 || N % 3 == 0) {
     if constexpr (N > 384 || (!PAD && N % 3 != 0 && N > 256)) return cudaErrorInvalidValue;
+    else if constexpr (sizeof(R) == 8 && PAD)
+      return p3s_run<R, PAD, N, 4>(p, nl, maxbits, st);  // 50-53 KB of shared memory per warp
     else return p3s_run<R, PAD, N, TuneC<N, R>::WS>(p, nl, maxbits, st);
   } else if constexpr (N > 256) {
     return cudaErrorInvalidValue;
@@ -1266,7 +1267,7 @@ static cudaError_t pass_t(FusedPlan* p, int pass, const void* uhat, void* nl,
                           unsigned long long* maxbits, cudaStream_t st) {
   using C = cx<R>;
   C* nlp = p->pad ? (C*)p->nlM : (C*)nl;
-  if constexpr (sizeof(R) == 4) {
+  {
     if (p->pad) {
       switch (pass) {
         case 1: {
@@ -1390,8 +1391,13 @@ cudaError_t fused_update(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, co
 
 cudaError_t fused_update(FusedPlan* p, const UpdateArgs<double>& U, int ncomp, const void* nl,
                          cudaStream_t st) {
-  if (!p || p->prec != 1 || p->pad || !tw_base<double>()) return cudaErrorNotReady;
+  if (!p || p->prec != 1 || !tw_base<double>()) return cudaErrorNotReady;
   if (p->dim == 2) return fused2d_update<double>(p->f2, U, ncomp, (const double2*)nl, st);
+  if (p->pad) {
+#define PF_CALL(NN) p5_n<double, NN, true>(p, U, ncomp, (const double2*)p->nlM, st)
+    PF_SWITCH_M(p->f.t0, PF_CALL)
+#undef PF_CALL
+  }
 #define PF_CALL(NN) p5_n<double, NN, false>(p, U, ncomp, (const double2*)nl, st)
   PF_SWITCH_S(p->f.n0, PF_CALL)
 #undef PF_CALL

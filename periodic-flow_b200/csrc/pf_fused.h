@@ -8,9 +8,9 @@ namespace pf {
 struct FusedPlan;
 
 // Returns nullptr when no fused schedule is built for this geometry (3D:
-// FP32 2/3 rule, sides 2^b 16..512 with n2 <= 256 and 3 * 2^b 48..384; FP32
-// 3/2 rule and FP64 2/3 rule, sides 2^b 16..256; 2D: 2/3 rule, FP32 and
-// FP64, sides 2^b 16..1024).  2D plans run passes 1 and 3 and the update;
+// FP32 2/3 rule, sides 2^b 16..512 with n2 <= 256 and 3 * 2^b 48..384; 3/2
+// rule (FP32, FP64) and FP64 2/3 rule, sides 2^b 16..256; 2D: 2/3 rule, FP32
+// and FP64, sides 2^b 16..1024).  2D plans run passes 1 and 3 and the update;
 // passes 2 and 4 are no-ops there.
 FusedPlan* fused_create(const Geo& g, int precision, int dealias);
 void fused_destroy(FusedPlan* p);

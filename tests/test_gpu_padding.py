@@ -121,3 +121,52 @@ def test_fused_padded_256_matches_generic():
         out.append(s.space_solver.u_hat)
         del s
     assert rel_l2(out[0], out[1]) < 2e-6
+
+
+# ------------------------------------------------- fused 3/2 schedule (FP64)
+@pytest.mark.parametrize("N", [(16, 16, 16), (32, 64, 32), (64, 32, 128), (128, 64, 32)])
+@pytest.mark.parametrize("integ", ["rk3", "rk4", "implicit_pc"])
+def test_fused_padded_fp64_vs_oracle(N, integ):
+    """FP64 fused passes on the padded grid (the reference's precision and
+    default rule) vs the FP64 oracle, 2 steps."""
+    o = O.OracleSolver(N, 2e-3, time_integrator=integ, viscosity=2e-3, dealias="3/2")
+    uh0 = O.spectral_random_field(o.grid, 6)
+    o.initialize(uh0, "fourier")
+    s = solver(N, 2e-3, time_integrator=integ, viscosity=2e-3, precision="fp64", fused=True)
+    s.initialize(uh0, "fourier")
+    o.advance(2)
+    s.space_solver.step(2)
+    assert rel_l2(s.space_solver.u_hat, o.u_hat) < 1e-11
+
+
+def test_fused_padded_fp64_forcing_cfl_noise_matches_generic():
+    N = (64, 64, 64)
+    kw = dict(time_integrator="rk3", viscosity=2e-3, precision="fp64",
+              forcing=(0.1, 2.5), cfl=0.5, noise_mag=1e-3, seed=3)
+    a = solver(N, 1e-3, fused=True, **kw)
+    b = solver(N, 1e-3, fused=False, **kw)
+    uh0 = O.spectral_random_field(O.Grid(N), 1)
+    a.initialize(uh0, "fourier")
+    b.initialize(uh0, "fourier")
+    a.space_solver.step(3)
+    b.space_solver.step(3)
+    ta, sa, da = a.space_solver.time()
+    tb, sb, db = b.space_solver.time()
+    assert sa == sb == 3 and abs(da - db) < 1e-12 * db
+    assert rel_l2(a.space_solver.u_hat, b.space_solver.u_hat) < 1e-12
+
+
+def test_fused_padded_fp64_256_matches_generic():
+    """FP64 384-point padded passes at 256^3: fused and generic agree after
+    one RK3 step."""
+    N = (256, 256, 256)
+    kw = dict(time_integrator="rk3", viscosity=2e-3, precision="fp64", cfl=0.5)
+    uh0 = O.spectral_random_field(O.Grid(N), 2)
+    out = []
+    for fused in (True, False):
+        s = solver(N, 1e-3, fused=fused, **kw)
+        s.initialize(uh0, "fourier")
+        s.space_solver.step(1)
+        out.append(s.space_solver.u_hat)
+        del s
+    assert rel_l2(out[0], out[1]) < 1e-12
