@@ -111,6 +111,28 @@ def test_served_results_equal_alone():
         assert rel_l2(mixed[r.rid], r.result) < 1e-6, r
 
 
+def test_nonlinear_points_cap():
+    """With the cap at one request's points the nonlinear requests run one
+    after another in arrival order, a linear one passes them, and results
+    equal the serial run's."""
+    from periodicflow.serving import Request, Server
+    reqs = [Request(0, 0.0, "tgv", (32, 32, 32), 60),
+            Request(1, 0.0, "tgv", (64, 64), 60),
+            Request(2, 0.0, "thermal", (64, 64), 100, seed=1),
+            Request(3, 0.0, "tgv", (32, 32, 32), 40)]
+    srv = Server(chunk_nonlinear=15, chunk_linear=50, keep_results=True,
+                 nl_points_cap=32 ** 3)
+    m = srv.run(reqs, "continuous")
+    assert m["requests"] == 4
+    mixed = {r.rid: r.result for r in reqs}
+    assert reqs[1].admitted >= reqs[0].finished
+    assert reqs[3].admitted >= reqs[1].finished
+    assert reqs[2].admitted < reqs[0].finished
+    srv.run(reqs, "serial")
+    for r in reqs:
+        assert rel_l2(mixed[r.rid], r.result) < 1e-6, r
+
+
 def test_admission_respects_budget():
     from periodicflow.serving import Request, Server
     reqs = [Request(i, 0.0, "thermal", (128, 128), 20, seed=i) for i in range(4)]
