@@ -11,7 +11,7 @@
  * Reference interfaces replaced (paths inside the periodic-flow project):
  *   Solver.__init__            src/periodicflow/simulation.py:56-114
  *   SpaceSolver.__init__       src/periodicflow/space_solver.py:107-150
- *   FourierSpace.__init__      src/periodicflow/basis.py:87-145
+ *   FourierSpace.__init__      src/periodicflow/basis.py:34-92
  *   Solver.initialize          src/periodicflow/simulation.py:161-180
  *   initialize_velocity        src/periodicflow/space_solver.py:180-213
  *   forward / backward         src/periodicflow/space_solver.py:215-225
@@ -54,22 +54,22 @@ extern "C" {
 #define PF_NOISE_SRC_PHILOX 1   /* counter-based, Hermitian-symmetric draws */
 #define PF_NOISE_SRC_INJECTED 2 /* caller supplies w1, w2 every step */
 
-#define PF_DEALIAS_TRUNCATE 0 /* '2/3' / 'truncate' (basis.py:135-136) */
-#define PF_DEALIAS_PAD 1      /* '3/2' / 'pad' (basis.py:133-134) */
+#define PF_DEALIAS_TRUNCATE 0 /* '2/3' / 'truncate' (basis.py:82-83) */
+#define PF_DEALIAS_PAD 1      /* '3/2' / 'pad' (basis.py:80-81) */
 
 #define PF_FP32 0
 #define PF_FP64 1
 
 typedef struct pf_config {
   int dim;                /* 2 or 3 */
-  int n[3];               /* grid points per axis (power of two, 4..1024) */
+  int n[3];               /* grid points per axis: 2^b 4..1024 or 3 * 2^b 12..768 */
   double domain[3][2];    /* (start, end) per axis */
   int is_nonlinear;       /* simulation.py:61 */
   int integrator;         /* PF_EXPLICIT_PC .. PF_RK4 */
   double viscosity;       /* L = -viscosity |k|^2 (space_solver.py:147) */
   int noise_type;         /* PF_NOISE_THERMAL / PF_NOISE_CORRELATED */
   double noise_mag;       /* 0 disables the noise term */
-  int dealias;            /* PF_DEALIAS_TRUNCATE */
+  int dealias;            /* PF_DEALIAS_TRUNCATE or PF_DEALIAS_PAD */
   int mask_nyquist;       /* zero Nyquist modes of the nonlinear term */
   int precision;          /* PF_FP32 / PF_FP64 */
   double dt;

@@ -44,20 +44,20 @@ FFT_WORKERS = None  # None -> scipy default (1); bench sets os.cpu_count()
 
 
 # ----------------------------------------------------------------------------
-# Discretisation: basis.py:87-145
+# Discretisation: basis.py:34-92
 # ----------------------------------------------------------------------------
 class Grid:
     """Wavenumbers, masks and transforms of one periodic box.
 
-    Restates basis.py:103-130 (domain parsing, wavenumbers, k2, k/k^2) and the
-    dealias rule table of basis.py:132-145 for the '2/3' / 'truncate' rule.
+    Restates basis.py:50-77 (domain parsing, wavenumbers, k2, k/k^2) and the
+    dealias rule table of basis.py:79-92 for the '2/3' / 'truncate' rule.
     """
 
     def __init__(self, N, domain=2 * np.pi, dealias="2/3", mask_nyquist=False):
         N = [int(n) for n in N]
         self.N = N
         self.dim = len(N)
-        # basis.py:103-113
+        # basis.py:50-60
         if isinstance(domain, float):
             self.domain = [(0, domain) for _ in range(self.dim)]
         elif isinstance(domain, (list, tuple)):
@@ -87,7 +87,7 @@ class Grid:
             shp[ax] = kk.size
             kint.append(kk.reshape(shp))
         self.kint1d = kint
-        # basis.py:118,128-130: scaled, broadcast wavenumbers
+        # basis.py:65,75-77: scaled, broadcast wavenumbers
         self.k = np.array([np.broadcast_to(kint[ax] * (2 * np.pi / self.lengths[ax]),
                                            self.spec_shape) for ax in range(d)])
         self.k2 = np.sum(self.k ** 2, axis=0)
@@ -99,7 +99,7 @@ class Grid:
         for ax in range(d):
             keep = keep & (3 * np.abs(kint[ax]) < N[ax])
         self.dealias_mask = keep.astype(np.float64)
-        # basis.py:125 get_mask_nyquist
+        # basis.py:72 get_mask_nyquist
         if mask_nyquist:
             nyq = np.ones(self.spec_shape, dtype=bool)
             for ax in range(d):
@@ -112,7 +112,7 @@ class Grid:
             self.nyquist_mask = nyq.astype(np.float64)
         else:
             self.nyquist_mask = None
-        # basis.py:127 local_mesh: x_j = a + L j / N, sparse broadcastable arrays
+        # basis.py:74 local_mesh: x_j = a + L j / N, sparse broadcastable arrays
         self.x = []
         for ax in range(d):
             a, _ = self.domain[ax]
@@ -142,7 +142,7 @@ class Grid:
     def backward_dealiased(self, uh):
         """Vp.backward / Wp.backward of space_solver.py:284,291.
 
-        '2/3': backward of the truncated copy.  '3/2' (basis.py:133-134): the
+        '2/3': backward of the truncated copy.  '3/2' (basis.py:80-81): the
         spectrum padded onto M = 3N/2 per axis (Nyquist modes of even sides
         split in half between +N/2 and -N/2; halved on the last axis), then the
         unnormalised backward transform on the M grid.

@@ -240,7 +240,7 @@ static cudaError_t forward_into(pf_solver* h, const R* P, cx<R>* X, int nc) {
   return forward_g<R>(h, h->g, P, X, nc);
 }
 
-// 3/2 rule (basis.py:133-134): u and omega = i k x u padded onto the M = 3N/2
+// 3/2 rule (basis.py:80-81): u and omega = i k x u padded onto the M = 3N/2
 // grid, u x omega there, forward transform normalised by 1 / prod M, then
 // truncated back to the N grid, unprojected, into h->nl
 template <typename R>
@@ -595,7 +595,7 @@ static int validate(const pf_config* c) {
     if (!fft_length_supported(c->n[a]))
       return fail(nullptr, PF_ERR_UNSUPPORTED,
                   "grid size " + std::to_string(c->n[a]) +
-                      " not built: powers of two from 4 to 1024 are supported");
+                      " not built: sides 2^b from 4 to 1024 and 3 * 2^b from 12 to 768 are supported");
     if (!(c->domain[a][1] > c->domain[a][0]))
       return fail(nullptr, PF_ERR_INVALID, "Invalid domain.");
   }

@@ -94,7 +94,7 @@ struct FGeo {
 // 2/3 rule (PAD false, t == n): rows with |k| <= kmax are kept.  3/2 rule
 // (PAD true, t = 3n/2): the N-grid spectrum embedded in the t grid, the even
 // side's Nyquist row (wavenumber -n/2) split half to +n/2 and half to -n/2
-// (basis.py:133-134 padding).  Its N-grid row index is kf mod n.
+// (basis.py:80-81 padding).  Its N-grid row index is kf mod n.
 template <bool PAD> PF_D float row_weight(int i, int t, int n, int kmax, int& kf) {
   if constexpr (!PAD) {
     kf = kfreq(i, t);

@@ -104,7 +104,7 @@ extern "C" int pf_backward_noalloc(int precision, int dim, const int* n, const v
     if (!fft_length_supported(n[a]))
       return set_static_error(PF_ERR_UNSUPPORTED,
                               "pf_backward_noalloc: grid size " + std::to_string(n[a]) +
-                                  " not built: powers of two from 4 to 1024 are supported");
+                                  " not built: sides 2^b from 4 to 1024 and 3 * 2^b from 12 to 768 are supported");
     nspec *= (a == dim - 1) ? (n[a] / 2 + 1) : n[a];
   }
   const size_t cbytes = precision == PF_FP64 ? 16 : 8;

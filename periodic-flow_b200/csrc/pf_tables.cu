@@ -17,9 +17,13 @@ long long launch_total() { return g_launches.load(std::memory_order_relaxed); }
 static __device__ float2 g_tw_f32[kTwSize];
 static __device__ double2 g_tw_f64[kTwSize];
 
-// device addresses of the tables, per device
-static std::vector<const float2*> s_tw32;
-static std::vector<const double2*> s_tw64;
+// Device addresses of the tables, one slot per device.  Fixed arrays of
+// atomics: tw_base() reads a slot without the set-up mutex while another host
+// thread may be setting up a different device, so nothing here is ever
+// reallocated.
+constexpr int kMaxDevices = 64;
+static std::atomic<const float2*> s_tw32[kMaxDevices];
+static std::atomic<const double2*> s_tw64[kMaxDevices];
 
 // exp(-2 pi i m / n) in FP64, evaluated on the first octant and mapped by
 // symmetry so every entry is as accurate as the host sin/cos near zero.
@@ -46,12 +50,13 @@ static void root_of_unity(long m, long n, double* c, double* s) {
 
 cudaError_t ensure_tables() {
   static std::mutex mu;
-  static std::vector<int> done;  // per device
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lk(mu);
-  if ((int)done.size() > dev && done[dev]) return cudaSuccess;
+  if (s_tw32[dev].load(std::memory_order_acquire) && s_tw64[dev].load(std::memory_order_acquire))
+    return cudaSuccess;
   std::vector<float2> f(kTwSize);
   std::vector<double2> d(kTwSize);
   auto fill = [&](int n) {
@@ -75,26 +80,20 @@ cudaError_t ensure_tables() {
   if (e != cudaSuccess) return e;
   e = cudaGetSymbolAddress(&p64, g_tw_f64);
   if (e != cudaSuccess) return e;
-  if ((int)done.size() <= dev) {
-    done.resize(dev + 1, 0);
-    s_tw32.resize(dev + 1, nullptr);
-    s_tw64.resize(dev + 1, nullptr);
-  }
-  s_tw32[dev] = (const float2*)p32;
-  s_tw64[dev] = (const double2*)p64;
-  done[dev] = 1;
+  s_tw64[dev].store((const double2*)p64, std::memory_order_release);
+  s_tw32[dev].store((const float2*)p32, std::memory_order_release);
   return cudaSuccess;
 }
 
 template <> const float2* tw_base<float>() {
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev >= (int)s_tw32.size()) return nullptr;
-  return s_tw32[dev];
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+  return s_tw32[dev].load(std::memory_order_acquire);
 }
 template <> const double2* tw_base<double>() {
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev >= (int)s_tw64.size()) return nullptr;
-  return s_tw64[dev];
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+  return s_tw64[dev].load(std::memory_order_acquire);
 }
 
 }  // namespace pf

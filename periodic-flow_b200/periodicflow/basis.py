@@ -1,4 +1,4 @@
-"""Host-side description of the periodic box (the reference's basis.py:63-145).
+"""Host-side description of the periodic box (the reference's basis.py:10-92).
 
 The device computes wavenumbers from mode indices; the arrays built here are
 the host views the reference exposes (``x``, ``k``, ``k2``, ``k_over_k2``,
@@ -12,7 +12,7 @@ DEALIAS_RULES = {"3/2": "pad", "pad": "pad", "2/3": "truncate", "truncate": "tru
 
 
 def parse_domain(domain, dim):
-    """Domain forms accepted by basis.py:103-113."""
+    """Domain forms accepted by basis.py:50-60."""
     if isinstance(domain, float):
         return [(0.0, domain) for _ in range(dim)]
     if isinstance(domain, (list, tuple)):

@@ -52,8 +52,9 @@ class Request:
 
 
 # physical set-up of the two kinds of request.  Thermal runs use the implicit
-# predictor-corrector: the explicit one is unstable once nu |k|^2 dt > 2
-# (|k| > 14 at nu = 0.1, dt = 0.01), i.e. on every grid served here.
+# predictor-corrector: the explicit one (amplification 1 + z + z^2/2, z =
+# -nu |k|^2 dt) is unstable once nu |k|^2 dt > 2, i.e. |k| > sqrt(2 / (nu dt))
+# = 44.7 at nu = 0.1, dt = 0.01, which every grid from 128^2 up contains.
 TGV = dict(dt=0.005, integrator="rk4", nu=1 / 1600)
 THERMAL = dict(dt=0.01, integrator="implicit_pc", nu=0.1, kT=1e-3)
 

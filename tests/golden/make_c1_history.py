@@ -13,7 +13,7 @@ leray_projection, apply_linear_operator) and periodicflow.time_integrator
 (RK4, Numba path), unchanged, with the glue of make_golden.py (scipy.fft in
 place of shenfun).  Needs the reference checkout and numba:
 
-    python tests/golden/make_c1_history.py [--ref /root/reference]
+    python tests/golden/make_c1_history.py --ref <periodic-flow checkout>
 """
 from __future__ import annotations
 
@@ -30,7 +30,9 @@ from make_golden import Box, load_reference  # noqa: E402
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("PERIODICFLOW_REF"),
+                    required="PERIODICFLOW_REF" not in os.environ,
+                    help="root of a periodic-flow checkout (or set PERIODICFLOW_REF)")
     ap.add_argument("--steps", type=int, default=400)
     args = ap.parse_args()
     rmath, rti, _ = load_reference(args.ref)

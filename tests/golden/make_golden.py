@@ -1,9 +1,9 @@
 """Generate the golden fixtures under tests/golden/ from the reference's own code.
 
 Run in a container that has the reference checkout (it is read from
-``--ref``, default /root/reference) and numba:
+``--ref`` or the PERIODICFLOW_REF environment variable) and numba:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <periodic-flow checkout>
 
 What runs is the reference's code, unchanged:
   * ``periodicflow.math``            (cross, curl, apply_linear_operator,
@@ -16,7 +16,7 @@ What runs is the reference's code, unchanged:
     and mpi4py, which are not installable here) and compiled with numba.
 
 shenfun, mpi4py and h5py are absent, so the glue around those kernels is
-restated here, independently of oracle/: wavenumbers (basis.py:115-130),
+restated here, independently of oracle/: wavenumbers (basis.py:62-77),
 normal factor (space_solver.py:143-147), random_fields RNG order
 (space_solver.py:227-238), compute_rhs (space_solver.py:273-310) and the solve
 loop body (simulation.py:205-213), with scipy.fft standing in for shenfun's
@@ -175,7 +175,9 @@ def random_solenoidal(box, seed, amp=1.0):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("PERIODICFLOW_REF"),
+                    required="PERIODICFLOW_REF" not in os.environ,
+                    help="root of a periodic-flow checkout (or set PERIODICFLOW_REF)")
     args = ap.parse_args()
     rmath, rti, rnoise = load_reference(args.ref)
     rng = np.random.default_rng(20240601)

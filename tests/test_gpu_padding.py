@@ -1,5 +1,5 @@
 """GPU parity of the 3/2 (padding) dealias rule against the oracle's
-restatement (the reference's default rule, basis.py:133-134; shenfun's own
+restatement (the reference's default rule, basis.py:80-81; shenfun's own
 padding is not available here, so the convention is the oracle's: Nyquist
 modes split in half on padding and folded on truncation)."""
 import numpy as np
