@@ -228,8 +228,15 @@ def run_ours(args, dist, rank, world):
         e2e = run_e2e(args, uh0, rank, dist, args.dealias)
     # ------------------------------------------------------------ cpu baseline
     cpu = None
+    check = None
     if rank == 0 and world == 1 and not args.no_cpu and not pad:
-        cpu = cpu_baseline(n, args.cpu_steps)
+        cpu, oracle_state = cpu_baseline(n, args.cpu_steps, uh0)
+        check = oracle_check(n, uh0, oracle_state, args.cpu_steps)
+        del oracle_state
+        check["config2_stokes_256sq"] = {
+            "workload": "2D thermal Stokes 256^2, explicit PC dt 0.01, injected NumPy noise "
+                        "(seed 0), 10 steps, relative L2 vs FP64 oracle",
+            "fp32_rel_l2": oracle_check_stokes("fp32"), "fp64_rel_l2": oracle_check_stokes("fp64")}
     ensemble = None
     if rank == 0 and not args.no_ensemble and not pad:
         ensemble = run_ensemble(args)
@@ -260,7 +267,8 @@ def run_ours(args, dist, rank, world):
                        "dt_after_run": dt_now},
             "gpu_launches": int(c1.value - c0.value),
             "clocks": ck, "roofline": roofline, "step_roofline": step_roof,
-            "e2e": e2e, "cpu_baseline": cpu, "batched": ensemble, "padded_3_2": padded,
+            "e2e": e2e, "cpu_baseline": cpu, "oracle_check": check,
+            "batched": ensemble, "padded_3_2": padded,
             "cufft_comparison": cufft, "fp64": fp64,
         }
         print(json.dumps(line), flush=True)
@@ -604,22 +612,87 @@ def run_serving(args):
     return out
 
 
-def cpu_baseline(n, steps):
-    """The oracle (FP64 NumPy + scipy.fft on all host cores) on the same box."""
+def cpu_baseline(n, steps, uh0):
+    """The oracle (FP64 NumPy + scipy.fft on all host cores) on the same box,
+    from the benchmark's initial field.  Returns the baseline record and the
+    oracle, whose state the FP32 check below compares against."""
     import scipy.fft  # noqa: F401
     import oracle as O
     import oracle.pf_oracle as P
     P.FFT_WORKERS = os.cpu_count()
     o = O.OracleSolver((n, n, n), CFG["dt0"], time_integrator=CFG["integrator"],
                        viscosity=CFG["nu"], forcing=CFG["forcing"], cfl=CFG["cfl"])
-    o.initialize(oracle_initial_field(n, CFG["seed"]), "fourier")
+    o.initialize(uh0, "fourier")
     t0 = time.perf_counter()
     o.advance(steps)
     sec = time.perf_counter() - t0
     return {"value": n ** 3 / 1e6 * steps / sec, "unit": UNIT, "cores": os.cpu_count(),
             "kind": "port", "sample": f"{steps} full RK3 steps of the {n}^3 workload, FP64 "
             f"oracle (NumPy pointwise single-threaded, scipy.fft workers={os.cpu_count()}), "
-            f"{sec:.1f} s"}
+            f"{sec:.1f} s"}, o
+
+
+def spectrum_errors(got, ref):
+    """Max relative error over shells holding >= 1e-10 of the peak shell
+    energy (the initial spectrum underflows to 0 at high k), and the relative
+    L2 error of the whole spectrum."""
+    got, ref = np.asarray(got, float), np.asarray(ref, float)
+    m = min(len(got), len(ref))
+    got, ref = got[:m], ref[:m]
+    sel = ref >= 1e-10 * ref.max()
+    rel = np.abs(got[sel] - ref[sel]) / ref[sel]
+    return float(rel.max()), float(np.linalg.norm(got - ref) / np.linalg.norm(ref)), int(sel.sum())
+
+
+def oracle_check(n, uh0, o, steps):
+    """The headline workload in FP32 through the fused schedule, advanced from
+    the same initial field by the oracle's steps, against the FP64 oracle."""
+    import oracle as O
+    sol = make_solver(n)
+    ss = sol.space_solver
+    ss.initialize_velocity(uh0, "fourier")
+    ss.step(steps)
+    got = ss.u_hat
+    rel = float(np.linalg.norm(got - o.u_hat) / np.linalg.norm(o.u_hat))
+    nb = int(np.sqrt(3 * (n // 2) ** 2)) + 2
+    smax, sl2, nsel = spectrum_errors(ss.spectrum(nb), O.spectrum(o.grid, o.u_hat, nb))
+    _, _, dt = ss.time()
+    out = {"workload": f"{n}^3 forced turbulence (seed-1 field, RK3 CFL 0.5, band forcing), "
+                       "FP32 fused schedule vs FP64 oracle from the same initial field",
+           "steps": steps, "rel_l2": rel, "tolerance": 1e-5,
+           "spectrum_max_rel_err": smax, "spectrum_shells_compared": nsel,
+           "spectrum_rel_l2": sl2, "dt_rel_err": abs(dt - o.dt) / o.dt}
+    del sol
+    return out
+
+
+def oracle_check_stokes(precision, steps=10):
+    """Configuration 2 (2D thermal Stokes 256^2, nu 0.1, kT 1e-3, explicit PC,
+    dt 0.01) for `steps` steps with the reference's NumPy draws (seed 0)
+    injected into both codes.  The explicit scheme is unstable at 256^2
+    (nu |k|^2 dt up to 33 > 2), so the state grows each step; the check is of
+    the arithmetic, relative L2 over all modes."""
+    import oracle as O
+    from periodicflow import simulation as sim
+    n, nu, kT, dt = 256, 0.1, 1e-3, 0.01
+    mag = float(np.sqrt(2 * nu * kT))
+    g = O.Grid((n, n))
+    rng = np.random.RandomState(0)
+    fields = [O.numpy_noise_fields(g, "thermal", rng) for _ in range(steps)]
+    o = O.OracleSolver((n, n), dt, is_nonlinear=False, time_integrator="explicit_pc",
+                       viscosity=nu, noise_type="thermal", noise_mag=mag,
+                       noise=lambda step: fields[step - 1])
+    o.initialize(np.zeros((2,) + g.spec_shape, complex), "fourier")
+    o.advance(steps)
+    s = sim.Solver([n, n], dt, 1.0, is_nonlinear=False, time_integrator="explicit_pc",
+                   viscosity=nu, noise_type="thermal", noise_mag=mag, precision=precision,
+                   noise_source="injected")
+    ss = s.space_solver
+    for w1, w2 in fields:
+        ss.inject_noise(w1, w2)
+        ss.step(1)
+    got = ss.u_hat
+    return float(np.linalg.norm(got - o.u_hat) / np.linalg.norm(o.u_hat))
 
 
 def run_reference(args, rank, world):

@@ -133,8 +133,8 @@ int pf_graph_replay(pf_solver* h);
 
 /* Autotuner (no reference counterpart; the reference has one CPU schedule):
  * times every launch variant of the fused passes 1-4 (radix width, columns
- * per CTA, register cap, staging depth) on this solver's buffers and keeps
- * the fastest; later solvers of the same geometry (precision, dealias rule,
+ * per CTA, register cap, staging depth, values per lane) inside the chain of
+ * passes 1-4 on this solver's buffers and keeps the fastest; later solvers of the same geometry (precision, dealias rule,
  * sides) in this process start from the picks.  Leaves the state unchanged;
  * synchronous; not inside a graph capture.  picks (12 ints, may be NULL):
  * variants of passes 0..5 for 256-point axes, then for 384-point axes.
@@ -156,6 +156,28 @@ int pf_history(pf_solver* h, double* out, int max_steps, int* count);
 int pf_record_history(pf_solver* h, int enable);
 /* Shell spectrum E(k), nbins bins of width 2 pi / L0. */
 int pf_spectrum(pf_solver* h, double* out, int nbins);
+
+/* SpaceSolver.compute_rhs(a) (space_solver.py:302-310) on the current state,
+ * into arrays of the solver read back with pf_get_rhs (the time step itself
+ * fuses these terms into the stage update and never stores them):
+ *   PF_RHS_LINEAR     L u_hat                          (space_solver.py:273-277)
+ *   PF_RHS_NONLINEAR  P[F(u x omega)], Nyquist-masked if configured; zero for
+ *                     linear solvers                   (space_solver.py:279-300)
+ *   PF_RHS_NOISE      noise_mag P[xi(w1 + a w2)] with the noise fields of the
+ *                     next step (Philox draws keyed by it, or the last
+ *                     injected w1, w2)                 (space_solver.py:240-265)
+ *   PF_RHS_FORCING    the band forcing (zero without)  (space_solver.py:267-271)
+ *   PF_RHS_P_HAT      (k/k^2).xi before the noise_mag scale: the output of the
+ *                     last Leray projection of compute_rhs, as the reference
+ *                     leaves p_hat; zero when noise_mag is 0 (no draws)
+ * Arrays are (dim, spectral) complex128, p_hat (spectral).  Synchronous. */
+#define PF_RHS_LINEAR 0
+#define PF_RHS_NONLINEAR 1
+#define PF_RHS_NOISE 2
+#define PF_RHS_FORCING 3
+#define PF_RHS_P_HAT 4
+int pf_compute_rhs(pf_solver* h, double a);
+int pf_get_rhs(pf_solver* h, int which, double* out, int where);
 
 /* ---- measurement ------------------------------------------------------- */
 /* kernel passes that can be timed */

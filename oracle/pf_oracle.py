@@ -682,6 +682,43 @@ class OracleSolver:
         xi, _ = leray_projection(xi, g.k, g.k_over_k2)
         return xi * self.noise_mag
 
+    def _noise_fields_for(self, step):
+        """The noise fields advance() draws for time step `step` (1-based)."""
+        keep = self.step
+        self.step = step
+        try:
+            return self._noise_fields()
+        finally:
+            self.step = keep
+
+    def compute_rhs(self, a=0.0, w1=None, w2=None):
+        """space_solver.py:302-310 as separate arrays: rhs_linear (:273-277),
+        rhs_nonlinear (:279-300), noise and p_hat (:240-265; p_hat is the
+        output of add_noise's projection, the last one compute_rhs makes) and
+        forcing (new).  w1, w2 default to the next step's noise fields; with
+        noise_mag == 0 no fields are drawn and noise, p_hat are zero."""
+        g = self.grid
+        uh = self.u_hat
+        out = {"rhs_linear": apply_linear_operator(self.linear_operator, uh),
+               "rhs_nonlinear": (self.rhs_nonlinear(uh) if self.is_nonlinear
+                                 else np.zeros_like(uh))}
+        if self.noise_mag != 0.0:
+            if w1 is None:
+                w1, w2 = self._noise_fields_for(self.step + 1)
+            w = w1 + a * w2
+            if self.noise_type == "thermal":
+                xi = noise_divergence(symmetrize(w), g.k)
+            else:
+                xi = apply_linear_operator(self.correlation_func, w)
+            xi, p = leray_projection(xi, g.k, g.k_over_k2)
+            out["noise"], out["p_hat"] = xi * self.noise_mag, p
+        else:
+            out["noise"] = np.zeros_like(uh)
+            out["p_hat"] = np.zeros(g.spec_shape, dtype=np.complex128)
+        out["forcing"] = (linear_forcing(g, uh, *self.forcing_cfg)
+                          if self.forcing_cfg is not None else np.zeros_like(uh))
+        return out
+
     def advance(self, nsteps=1, diagnostics=False):
         """simulation.py:205-217 for a fixed number of steps."""
         g = self.grid
@@ -695,7 +732,11 @@ class OracleSolver:
             self.t += integ.dt
             self.step += 1
             u0 = self.u_hat.copy()
-            w1, w2 = self._noise_fields()
+            # noise_mag == 0 multiplies the noise by zero: counter-based draws
+            # are skipped (other sources still draw, keeping the reference's
+            # generator sequence)
+            skip = self.noise_mag == 0.0 and self.noise == "philox"
+            w1, w2 = (0.0, 0.0) if skip else self._noise_fields()
             Nl = np.zeros_like(self.u_hat)
             Lu = np.zeros_like(self.u_hat)
             for stage in range(integ.n_stages):
@@ -703,7 +744,8 @@ class OracleSolver:
                 Lu = apply_linear_operator(self.linear_operator, self.u_hat)
                 if self.is_nonlinear:
                     Nl = self.rhs_nonlinear(self.u_hat)
-                xi = self.noise_term(w1, w2, a)
+                xi = (self.noise_term(w1, w2, a) if self.noise_mag != 0.0
+                      else np.zeros_like(self.u_hat))
                 if self.forcing_cfg is not None:
                     f = linear_forcing(g, self.u_hat, *self.forcing_cfg)
                 else:

@@ -31,6 +31,20 @@ def _newest(paths):
     return max(os.path.getmtime(p) for p in paths)
 
 
+def _deps(dfile):
+    """Files listed in an nvcc -MD dependency file (None when missing or when a
+    listed file no longer exists, which forces a rebuild)."""
+    try:
+        text = open(dfile).read()
+    except OSError:
+        return None
+    body = text.split(":", 1)[1] if ":" in text else ""
+    files = [t for t in body.replace("\\\n", " ").split() if t != "\\"]
+    if not files or not all(os.path.exists(f) for f in files):
+        return None
+    return files
+
+
 def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
@@ -43,13 +57,16 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     for src in sources:
         obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
         objs.append(obj)
+        deps = _deps(obj[:-2] + ".d")
+        # headers this object was built from (all headers when unknown)
+        dep_time = _newest(deps) if deps is not None else hdr_time
         if force or not os.path.exists(obj) or os.path.getmtime(obj) < max(
-                os.path.getmtime(src), hdr_time):
+                os.path.getmtime(src), dep_time):
             todo.append((src, obj))
 
     def compile_one(item):
         src, obj = item
-        cmd = [NVCC] + ARCH + FLAGS + ["-c", src, "-o", obj]
+        cmd = [NVCC] + ARCH + FLAGS + ["-MD", "-MF", obj[:-2] + ".d", "-c", src, "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed on {src}:\n{r.stderr}")

@@ -34,6 +34,7 @@ struct pf_solver {
   void* lop = nullptr;    // nspec real (user L)
   void* corr = nullptr;   // nspec real (user C)
   void* winj = nullptr;   // 2 * ncomp * nspec complex
+  void* rhs = nullptr;    // pf_compute_rhs arrays: (4 d + 1) * nspec complex, on first use
   double* stage64 = nullptr;  // FP64 staging for transfers
   size_t stage64_elems = 0;
   double* dscal = nullptr;
@@ -702,7 +703,7 @@ int pf_destroy(pf_solver* h) {
   if (!h) return PF_OK;
   void* ptrs[] = {h->uhat, h->u0, h->nl, h->spec_tmp, h->phys_u, h->phys_w,
                   h->specM, h->physM_u, h->physM_w, h->lop,
-                  h->corr, h->winj, h->stage64, h->dscal, h->maxbits, h->hist_dev};
+                  h->corr, h->winj, h->rhs, h->stage64, h->dscal, h->maxbits, h->hist_dev};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->fused) fused_destroy(h->fused);
@@ -959,6 +960,76 @@ int pf_spectrum(pf_solver* h, double* out, int nbins) {
   cudaFree(tmp);
   if (e != cudaSuccess) return fail(h, PF_ERR_CUDA, std::string("pf_spectrum: ") + cudaGetErrorString(e));
   return PF_OK;
+}
+
+}  // extern "C"
+
+// compute_rhs(a) (space_solver.py:302-310) into h->rhs: the nonlinear term by
+// the per-operator path (the fused passes hand it to the update without an
+// axis-0 spectral copy), then every part per mode.
+template <typename R>
+static int compute_rhs_impl(pf_solver* h, double a) {
+  const Geo& g = h->g;
+  const size_t cb = 2 * h->rsz;
+  if (!h->rhs) PF_CUDA(h, cudaMalloc(&h->rhs, cb * ((size_t)4 * h->d + 1) * g.nspec));
+  if (h->cfg.is_nonlinear)
+    PF_CUDA(h, h->padded ? nonlinear_padded<R>(h, false) : nonlinear_generic<R>(h, false));
+  const bool forcing = h->cfg.forcing_eps > 0.0;
+  if (forcing)
+    PF_CUDA(h, launch_band_energy<R>((const cx<R>*)h->uhat, g,
+                                     h->cfg.forcing_kf * h->cfg.forcing_kf, h->dscal, h->st));
+  UpdateArgs<R> A;
+  memset(&A, 0, sizeof(A));
+  A.uhat = (cx<R>*)h->uhat;
+  A.u0 = (cx<R>*)h->u0;
+  A.nl = h->cfg.is_nonlinear ? (const cx<R>*)h->nl : nullptr;
+  A.lop = (const R*)h->lop;
+  A.corr = (const R*)h->corr;
+  A.winj = (const cx<R>*)h->winj;
+  A.dscal = h->dscal;
+  A.g = g;
+  A.coef.a = a;
+  A.nu = h->cfg.viscosity;
+  A.noise_mag = h->cfg.noise_mag;
+  A.noise_norm = noise_norm(h);
+  A.f_eps = h->cfg.forcing_eps;
+  A.f_kf2 = h->cfg.forcing_kf * h->cfg.forcing_kf;
+  A.seed = h->cfg.seed;
+  A.step = (uint64_t)(h->step + 1);  // the draws of the next step
+  A.noise_src = noise_src(h);
+  A.noise_type = h->cfg.noise_type;
+  A.nyq_mask = h->cfg.mask_nyquist;
+  A.forcing = forcing;
+  const long long f = (long long)h->d * g.nspec;
+  cx<R>* base = (cx<R>*)h->rhs;
+  RhsOut<R> o;
+  o.rhs_linear = base;
+  o.rhs_nonlinear = base + f;
+  o.noise = base + 2 * f;
+  o.forcing = base + 3 * f;
+  o.p_hat = base + 4 * f;
+  PF_CUDA(h, launch_rhs_parts<R>(A, h->ncomp, o, h->st));
+  PF_CUDA(h, cudaStreamSynchronize(h->st));
+  return PF_OK;
+}
+
+extern "C" {
+
+int pf_compute_rhs(pf_solver* h, double a) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  if (h->capturing) return fail(h, PF_ERR_INVALID, "pf_compute_rhs: not inside a graph capture");
+  return h->prec == PF_FP64 ? compute_rhs_impl<double>(h, a) : compute_rhs_impl<float>(h, a);
+}
+
+int pf_get_rhs(pf_solver* h, int which, double* out, int where) {
+  if (!h || !out) return fail(h, PF_ERR_INVALID, "pf_get_rhs: null argument");
+  if (which < PF_RHS_LINEAR || which > PF_RHS_P_HAT)
+    return fail(h, PF_ERR_INVALID, "pf_get_rhs: unknown array");
+  if (!h->rhs) return fail(h, PF_ERR_INVALID, "pf_get_rhs: call pf_compute_rhs first");
+  const size_t f = (size_t)h->d * h->g.nspec;
+  const size_t n = 2 * (which == PF_RHS_P_HAT ? (size_t)h->g.nspec : f);  // doubles
+  PF_CUDA(h, convert_out(h, (const char*)h->rhs + 2 * h->rsz * f * which, n));
+  return stage_out(h, out, n, where);
 }
 
 int pf_kernel_timer(pf_solver* h, int pass) {

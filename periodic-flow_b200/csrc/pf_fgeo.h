@@ -1,0 +1,29 @@
+// Geometry of the fused 3D pencil schedule, shared by pf_fused.cu and the
+// separately compiled pass kernels (pf_p3q.cu).
+#pragma once
+#include "pf_common.cuh"
+
+namespace pf {
+
+struct FGeo {
+  int n0, n1, n2, nh;          // N grid (the state's grid)
+  int t0, t1, t2;              // transform lengths: n_i (2/3 rule) or 3 n_i / 2 (3/2 rule)
+  int c1, c2;                  // compact inverse-input extents along axes 1, 2
+  int kmax0, kmax1, kmax2;
+  double ks0, ks1, ks2;
+  double cflw0, cflw1, cflw2;  // n_i / L_i
+  long long nspec;
+  int nlrow;                   // nl row stride along axis 0 (t1 nh)
+  long long nlcomp;            // nl component stride (t0 t1 nh)
+};
+
+// P3 of the 2/3 rule in FP32 with one shared-memory exchange per line FFT
+// (pf_p3q.cu): contiguous sides n2 = 128 or 256, W warps per CTA (6 or 7),
+// one CTA per SM, at most nsm CTAs.  B, nl, maxbits, err as for the other P3
+// forms.
+cudaError_t p3q_launch(int n2, int W, const float2* B, float2* nl, const FGeo& f,
+                       const float2* tw, unsigned long long* maxbits, float scale, int* err,
+                       long long ngroups, int nsm, cudaStream_t st);
+bool p3q_supported(int n2, int W);
+
+}  // namespace pf

@@ -24,9 +24,10 @@ cudaError_t fused_update(FusedPlan* p, const UpdateArgs<float>& U, int ncomp, co
 cudaError_t fused_update(FusedPlan* p, const UpdateArgs<double>& U, int ncomp, const void* nl,
                          cudaStream_t st);
 
-// Times every launch variant of passes 1-4 on this plan's buffers (each pass
-// writes only plan scratch and nl) and keeps the fastest; the picks (var[6],
-// var384[6]) also seed later plans of the same geometry.  Synchronous.
+// Times every launch variant of passes 1-4 inside the chain of passes 1-4 on
+// this plan's buffers (each pass writes only plan scratch and nl) and keeps
+// the fastest; the picks (var[6], var384[6]) also seed later plans of the
+// same geometry.  Synchronous.
 cudaError_t fused_autotune(FusedPlan* p, const void* uhat, void* nl, cudaStream_t st, int* picks);
 void fused_variants(const FusedPlan* p, int* out12);
 

@@ -42,6 +42,19 @@ template <typename R> struct StokesArgs {
   int first_stage;  // 1: skip a stage the next one never reads (implicit PC, linear)
 };
 
+// SpaceSolver.compute_rhs(a) outside the time step (space_solver.py:273-310):
+// the stage's parts written to separate arrays instead of being folded into
+// the update.  `A` supplies the state, L, C, noise source and forcing set-up
+// (A.coef.a is the stage's noise factor); nl is the unprojected nonlinear
+// term or nullptr.
+template <typename R> struct RhsOut {
+  cx<R>* rhs_linear;     // (d, nspec)
+  cx<R>* rhs_nonlinear;  // (d, nspec)
+  cx<R>* noise;          // (d, nspec)
+  cx<R>* forcing;        // (d, nspec)
+  cx<R>* p_hat;          // (nspec)
+};
+
 // What the ensemble batch needs to know about a member solver.
 struct SolverView {
   Geo g;
@@ -57,6 +70,9 @@ struct SolverView {
 };
 
 template <typename R> cudaError_t launch_update(const UpdateArgs<R>& A, int ncomp, cudaStream_t st);
+template <typename R>
+cudaError_t launch_rhs_parts(const UpdateArgs<R>& A, int ncomp, const RhsOut<R>& out,
+                             cudaStream_t st);
 template <typename R> cudaError_t launch_stokes(const StokesArgs<R>& A, int ncomp, cudaStream_t st);
 template <typename R>
 cudaError_t launch_mask_copy(cx<R>* dst, const cx<R>* src, const Geo& g, int ncomp, cudaStream_t st);

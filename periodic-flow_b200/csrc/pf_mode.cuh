@@ -80,22 +80,25 @@ template <int D> PF_D bool self_conjugate_plane(const Geo& g, const ModeIdx& ix)
   return il == 0 || ((nl % 2 == 0) && il == nl / 2);
 }
 
-// Leray projection of a D-vector: p = (k/k^2).v ; v -= p k (math.py:71-100)
+// Leray projection of a D-vector: p = (k/k^2).v ; v -= p k (math.py:71-100).
+// Returns p (the reference's p_hat output).
 template <typename R, int D>
-PF_D void leray(cx<R> (&v)[D], const R (&k)[D], R k2) {
+PF_D cx<R> leray(cx<R> (&v)[D], const R (&k)[D], R k2) {
   const R inv = k2 == R(0) ? R(0) : R(1) / k2;
   cx<R> p = czero<cx<R>>();
 #pragma unroll
   for (int a = 0; a < D; ++a) p = cadd(p, cscale(v[a], k[a] * inv));
 #pragma unroll
   for (int a = 0; a < D; ++a) v[a] = csub(v[a], cscale(p, k[a]));
+  return p;
 }
 
-// Noise of one stage from w = w1 + a w2 (space_solver.py:240-265).
-// thermal: xi_a = i sum_b k_b (W_ab + W_ba) sqrt(1/2); correlated: C w.
+// Unprojected, unscaled noise of one stage from w = w1 + a w2
+// (space_solver.py:240-265).  thermal: xi_a = i sum_b k_b (W_ab + W_ba)
+// sqrt(1/2); correlated: C w.
 template <typename R, int D, int NC>
-PF_D void noise_term(cx<R> (&xi)[D], const cx<R> (&w1)[NC], const cx<R> (&w2)[NC], R a,
-                     int noise_type, const R (&k)[D], R k2, R corr, R mag) {
+PF_D void noise_raw(cx<R> (&xi)[D], const cx<R> (&w1)[NC], const cx<R> (&w2)[NC], R a,
+                    int noise_type, const R (&k)[D], R corr) {
   if (noise_type == kThermal) {
     const R f = R(0.70710678118654752440);
 #pragma unroll
@@ -118,6 +121,13 @@ PF_D void noise_term(cx<R> (&xi)[D], const cx<R> (&w1)[NC], const cx<R> (&w2)[NC
       else xi[i] = czero<cx<R>>();
     }
   }
+}
+
+// Noise of one stage: noise_raw, Leray projection, times noise_mag.
+template <typename R, int D, int NC>
+PF_D void noise_term(cx<R> (&xi)[D], const cx<R> (&w1)[NC], const cx<R> (&w2)[NC], R a,
+                     int noise_type, const R (&k)[D], R k2, R corr, R mag) {
+  noise_raw<R, D, NC>(xi, w1, w2, a, noise_type, k, corr);
   leray<R, D>(xi, k, k2);
 #pragma unroll
   for (int i = 0; i < D; ++i) xi[i] = cscale(xi[i], mag);

@@ -18,6 +18,7 @@ PF_DEALIAS_TRUNCATE, PF_DEALIAS_PAD = 0, 1
 PF_FP32, PF_FP64 = 0, 1
 PF_PASS_UPDATE, PF_PASS_FFT_STRIDED, PF_PASS_FFT_LAST, PF_PASS_STOKES = 0, 1, 2, 4
 PF_PASS_FUSED = {1: 11, 2: 12, 3: 13, 4: 14, 5: 15}
+PF_RHS = {"rhs_linear": 0, "rhs_nonlinear": 1, "noise": 2, "forcing": 3, "p_hat": 4}
 
 
 class PfConfig(C.Structure):
@@ -80,6 +81,8 @@ _SIGS = [
     ("pf_history", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     ("pf_record_history", C.c_int, [C.c_void_p, C.c_int]),
     ("pf_spectrum", C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    ("pf_compute_rhs", C.c_int, [C.c_void_p, C.c_double]),
+    ("pf_get_rhs", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
     ("pf_kernel_timer", C.c_int, [C.c_void_p, C.c_int]),
     ("pf_kernel_timer_read", C.c_int, [C.c_void_p, C.POINTER(C.c_double),
                                        C.POINTER(C.c_longlong)]),

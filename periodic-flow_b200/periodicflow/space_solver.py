@@ -3,7 +3,8 @@
 The state lives on the GPU inside a C-ABI solver handle; ``u_hat`` and ``u``
 are host (NumPy, FP64) views materialised on access, and assignments upload.
 The right-hand side (nonlinear term, Leray projection, linear term, noise,
-forcing) is computed fused with the stage update on the device.
+forcing) is computed fused with the stage update on the device;
+``compute_rhs`` also writes its parts to arrays for callers that read them.
 """
 from __future__ import annotations
 
@@ -90,6 +91,8 @@ class SpaceSolver(FourierSpace):
         cfg = build_config(self.N, self.domain, is_nonlinear, integrator_id, viscosity,
                            noise_type, noise_mag, self.nyquist_mask is not None, precision, dt,
                            seed, noise_source, forcing, cfl, fused, dealias=self.dealias_rule)
+        self._u_host = None
+        self._rhs_ready = False
         h = C.c_void_p()
         N.check(N.lib().pf_create(C.byref(cfg), C.byref(h)), None, "pf_create")
         self._h = h
@@ -119,16 +122,22 @@ class SpaceSolver(FourierSpace):
 
     @property
     def u(self) -> np.ndarray:
-        """Physical velocity: backward transform of the current state."""
-        out = np.empty(self.shape_local_physical, dtype=np.float64)
-        N.check(N.lib().pf_get_physical(self._h, out.ctypes.data, 0), self._h, "get u")
-        return out
+        """Physical velocity: the backward transform of the current state,
+        written into this solver's host array (the same array object on every
+        access), so in-place edits of it reach the state through forward()."""
+        if self._u_host is None:
+            self._u_host = np.empty(self.shape_local_physical, dtype=np.float64)
+        N.check(N.lib().pf_get_physical(self._h, self._u_host.ctypes.data, 0), self._h, "get u")
+        return self._u_host
 
     @u.setter
     def u(self, value):
         a = np.ascontiguousarray(np.broadcast_to(value, self.shape_local_physical),
                                  dtype=np.float64)
         N.check(N.lib().pf_set_physical(self._h, a.ctypes.data, 0), self._h, "set u")
+        if self._u_host is None:
+            self._u_host = np.empty(self.shape_local_physical, dtype=np.float64)
+        self._u_host[...] = a
 
     # space_solver.py:180-213
     def initialize_velocity(self, u0, space: str = "physical", mask_zero_mode: bool = True):
@@ -155,9 +164,12 @@ class SpaceSolver(FourierSpace):
         N.check(N.lib().pf_project(self._h), self._h, "project")
 
     def forward(self, u=None):
-        """V.forward: physical -> spectral (space_solver.py:215-219)."""
-        if u is not None:
-            self.u = u
+        """V.forward (space_solver.py:215-219): the physical field -- ``u`` if
+        given, else this solver's host array ``self.u`` as last read or
+        edited in place -- transformed into the state."""
+        if u is None:
+            u = self._u_host if self._u_host is not None else self.u
+        self.u = u
 
     def backward(self):
         """V.backward (space_solver.py:221-225): returns the physical field."""
@@ -195,9 +207,30 @@ class SpaceSolver(FourierSpace):
         N.check(N.lib().pf_inject_noise(self._h, a.ctypes.data, b.ctypes.data, 0), self._h,
                 "inject_noise")
 
-    def compute_rhs(self, a: float = 0.0):  # pragma: no cover - documented gap
-        raise NotImplementedError(
-            "the right-hand side is fused with the stage update on the device; use Solver.solve")
+    def compute_rhs(self, a: float = 0.0):
+        """Assemble the right-hand side of the current state with noise factor
+        ``a`` (space_solver.py:302-310) into ``rhs_linear``, ``rhs_nonlinear``,
+        ``noise``, ``forcing`` and ``p_hat``.  The time step does not need
+        this call: on the device each stage computes these terms per mode
+        inside its update.  The noise uses the fields of the next step."""
+        N.check(N.lib().pf_compute_rhs(self._h, float(a)), self._h, "compute_rhs")
+        self._rhs_ready = True
+
+    def _rhs_array(self, name):
+        shape = self.shape_spectral if name == "p_hat" else self.shape_local_fourier
+        out = np.zeros(shape, dtype=np.complex128)
+        if self._rhs_ready:
+            N.check(N.lib().pf_get_rhs(self._h, N.PF_RHS[name], out.ctypes.data, 0), self._h,
+                    f"get {name}")
+        return out
+
+    # arrays of the reference's SpaceSolver (space_solver.py:152-178) as host
+    # copies of the last compute_rhs (zeros before it)
+    rhs_linear = property(lambda self: self._rhs_array("rhs_linear"))
+    rhs_nonlinear = property(lambda self: self._rhs_array("rhs_nonlinear"))
+    noise = property(lambda self: self._rhs_array("noise"))
+    forcing = property(lambda self: self._rhs_array("forcing"))
+    p_hat = property(lambda self: self._rhs_array("p_hat"))
 
     # ------------------------------------------------------------ diagnostics
     def energy(self):

@@ -330,9 +330,55 @@ def test_autotune_keeps_state_and_parity():
     before = a.space_solver.u_hat
     picks = a.space_solver.autotune()
     assert np.array_equal(a.space_solver.u_hat, before)
-    built = {1: range(0, 8), 2: range(0, 9), 3: range(0, 4), 4: range(0, 7)}
+    built = {1: range(0, 8), 2: range(0, 9), 3: range(0, 6), 4: range(0, 7)}
     assert all(picks["axes_256"][p] in built[p] for p in built)
     assert a.space_solver.fused_variants() == picks
+    a.space_solver.step(1)
+    ua = a.space_solver.u_hat
+    del a
+    b = solver(N, fused=False, **kw)
+    b.initialize(uh0, "fourier")
+    b.space_solver.step(1)
+    assert rel_l2(ua, b.space_solver.u_hat) < 2e-6
+
+
+@pytest.mark.parametrize("N,var", [((32, 32, 256), 4), ((32, 32, 256), 5), ((64, 32, 128), 4),
+                                   ((48, 96, 256), 4), ((128, 128, 128), 4)])
+def test_p3_one_exchange_form_vs_oracle(N, var, monkeypatch):
+    """P3 with sixteen values per lane (one exchange per line FFT, twiddles in
+    registers, shuffled output split, FP32 CFL sums): forcing + CFL vs the
+    FP64 oracle after 2 steps, and against the eight-value form."""
+    monkeypatch.setenv("PF_FUSED_VARIANT", f"p3:{var}")
+    kw = dict(dt=1e-3, time_integrator="rk3", viscosity=2e-3, precision="fp32",
+              forcing=(0.1, 2.5), cfl=0.5)
+    o = O.OracleSolver(N, 1e-3, time_integrator="rk3", viscosity=2e-3, forcing=(0.1, 2.5),
+                       cfl=0.5)
+    uh0 = O.spectral_random_field(o.grid, 5)
+    o.initialize(uh0, "fourier")
+    a = solver(N, fused=True, **kw)
+    assert a.space_solver.fused_variants()["axes_256"][3] == var
+    a.initialize(uh0, "fourier")
+    o.advance(2)
+    a.space_solver.step(2)
+    assert rel_l2(a.space_solver.u_hat, o.u_hat) < 1e-5
+    _, _, dt = a.space_solver.time()
+    assert abs(dt - o.dt) < 1e-5 * o.dt
+    monkeypatch.setenv("PF_FUSED_VARIANT", "p3:2")
+    b = solver(N, fused=True, **kw)
+    b.initialize(uh0, "fourier")
+    b.space_solver.step(2)
+    assert rel_l2(a.space_solver.u_hat, b.space_solver.u_hat) < 2e-6
+
+
+@pytest.mark.parametrize("var", [4, 5])
+def test_p3_one_exchange_form_256cubed_matches_generic(var, monkeypatch):
+    N = (256, 256, 256)
+    kw = dict(dt=1e-3, time_integrator="rk3", viscosity=2e-3, precision="fp32", cfl=0.5,
+              forcing=(0.1, 2.5))
+    uh0 = O.spectral_random_field(O.Grid(N), 4)
+    monkeypatch.setenv("PF_FUSED_VARIANT", f"p3:{var}")
+    a = solver(N, fused=True, **kw)
+    a.initialize(uh0, "fourier")
     a.space_solver.step(1)
     ua = a.space_solver.u_hat
     del a

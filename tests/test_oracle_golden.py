@@ -130,3 +130,37 @@ def test_oracle_tgv64_history_prefix():
     o.initialize(O.taylor_green(o.grid))
     h = np.array(o.advance(40, diagnostics=True))
     np.testing.assert_allclose(h, ref[:40], rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("kw", [
+    dict(N=(16, 16, 16), time_integrator="rk3", viscosity=2e-3, forcing=(0.1, 2.5)),
+    dict(N=(16, 8, 16), time_integrator="implicit_pc", viscosity=0.05, noise_type="thermal",
+         noise_mag=0.02, seed=3),
+    dict(N=(32, 16), time_integrator="explicit_pc", viscosity=0.01, noise_type="correlated",
+         noise_mag=0.1, mask_nyquist=True, seed=3),
+], ids=["3d_rk3_forcing", "3d_thermal", "2d_correlated_nyquist"])
+def test_oracle_compute_rhs_rebuilds_its_step(kw):
+    """compute_rhs(a) per stage fed to the integrator reproduces advance(1):
+    the arrays are the terms the reference's loop hands to stepping
+    (simulation.py:209-213)."""
+    kw = dict(kw)
+    N = kw.pop("N")
+    g = O.Grid(N, mask_nyquist=kw.get("mask_nyquist", False))
+    uh = O.spectral_random_field(g, 2)
+    a = O.OracleSolver(N, 0.01, **kw)
+    b = O.OracleSolver(N, 0.01, **kw)
+    if kw.get("noise_type") == "correlated":
+        C = np.exp(-g.k2 / 16.0)
+        a.set_correlation_function(C)
+        b.set_correlation_function(C)
+    a.initialize(uh, "fourier")
+    b.initialize(uh, "fourier")
+    a.advance(1)
+    integ = b.integrator
+    u0 = b.u_hat.copy()
+    w = b._noise_fields_for(1) if kw.get("noise_mag") else (None, None)
+    for stage in range(integ.n_stages):
+        r = b.compute_rhs(integ.noise_factor[stage], *w)
+        integ.stepping(b.u_hat, u0, stage, r["rhs_nonlinear"], r["rhs_linear"], r["forcing"],
+                       r["noise"])
+    assert rel_l2(b.u_hat, a.u_hat) < 1e-15
