@@ -240,6 +240,12 @@ def run_ours(args, dist, rank, world):
     ensemble = None
     if rank == 0 and not args.no_ensemble and not pad:
         ensemble = run_ensemble(args)
+    nlbatch = None
+    if rank == 0 and not args.no_nlbatch and not pad:
+        nlbatch = run_batched_nonlinear(args)
+    served = None
+    if rank == 0 and not args.no_serving and not pad:
+        served = run_serving(args)
     padded = None
     if rank == 0 and not args.no_padded and not pad:
         padded = run_padded(args, uh0, peak)
@@ -268,7 +274,8 @@ def run_ours(args, dist, rank, world):
             "gpu_launches": int(c1.value - c0.value),
             "clocks": ck, "roofline": roofline, "step_roofline": step_roof,
             "e2e": e2e, "cpu_baseline": cpu, "oracle_check": check,
-            "batched": ensemble, "padded_3_2": padded,
+            "batched": ensemble, "batched_nonlinear": nlbatch, "served": served,
+            "padded_3_2": padded,
             "cufft_comparison": cufft, "fp64": fp64,
         }
         print(json.dumps(line), flush=True)
@@ -603,12 +610,69 @@ def run_serving(args):
     reqs = poisson_requests(args.serve_requests, rate=50.0, seed=2,
                             max_steps=args.serve_max_steps)
     out = one(reqs, f"{len(reqs)} Poisson requests (50/s, seed 2): 2D 64^2-1024^2 and 3D "
-                    f"32^3-128^3 log-uniform, Taylor-Green or thermal noise, "
+                    f"32^3-192^3 log-uniform, Taylor-Green or thermal noise, "
                     f"100-{args.serve_max_steps} steps, 150 GB budget")
     small = poisson_requests(120, rate=200.0, seed=3, min_steps=100, max_steps=2000,
                              sizes2d=(64, 128, 256), sizes3d=(16, 32, 64))
     out["small_requests"] = one(small, "120 Poisson requests (200/s, seed 3): 2D 64^2-256^2 and "
                                        "3D 16^3-64^3, Taylor-Green or thermal noise, 100-2000 steps")
+    return out
+
+
+def run_batched_nonlinear(args):
+    """Realisations of a nonlinear configuration in one launch per fused pass
+    (pf_create_members) against the same boxes solved one at a time through
+    the plain solver (its one-step graph replayed per step), from the same
+    random initial fields; aggregate Mpts*steps/s, CUDA events."""
+    import torch
+    from periodicflow import _comm, simulation as sim
+    from periodicflow.basis import FourierSpace
+    from periodicflow.ensemble import Realisations
+    from periodicflow.initial import spectral_random_field
+    out = {}
+    cases = [("2D Taylor-Green-like random fields 256^2, RK4 dt 0.005, nu 1/1600, FP32",
+              (256, 256), 64, args.nlb_steps),
+             ("3D random fields 64^3, RK4 dt 0.005, nu 1/1600, FP32", (64, 64, 64), 32,
+              args.nlb_steps // 2)]
+    for label, N, M, steps in cases:
+        kw = dict(time_integrator="rk4", viscosity=1 / 1600, dealias="2/3", precision="fp32")
+        space = FourierSpace(_comm.COMM_WORLD, 0, list(N), dealias="2/3")
+        ics = [spectral_random_field(space, 100 + m) for m in range(M)]
+        R = Realisations(N, 0.005, M, **kw)
+        R.autotune()
+        for m, uh in enumerate(ics):
+            R.set_state(m, uh)
+        R.project()  # as Solver.initialize does
+        singles = []
+        for uh in ics:
+            s = sim.Solver(list(N), 0.005, 1.0, **kw)
+            s.initialize(uh, "fourier")
+            singles.append(s)
+        R.step(3)
+        for s in singles:
+            s.space_solver.step(3)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        R.step(steps)
+        e1.record()
+        torch.cuda.synchronize()
+        tb = e0.elapsed_time(e1) / 1e3
+        e0.record()
+        for s in singles:
+            s.space_solver.step(steps)
+        e1.record()
+        torch.cuda.synchronize()
+        tp = e0.elapsed_time(e1) / 1e3
+        diff = max(float(np.linalg.norm(R.state(m) - singles[m].space_solver.u_hat)
+                         / np.linalg.norm(singles[m].space_solver.u_hat)) for m in (0, M // 2, M - 1))
+        pts = M * float(np.prod(N)) / 1e6 * steps
+        out["2d" if len(N) == 2 else "3d"] = {
+            "workload": f"{M} x {label}, {steps} steps", "members": M, "steps": steps,
+            "batched_s": tb, "plain_s": tp, "batched_mpts_steps_per_s": pts / tb,
+            "plain_mpts_steps_per_s": pts / tp, "speedup_vs_plain": tp / tb,
+            "max_rel_diff_batched_vs_plain": diff}
+        del R, singles
     return out
 
 
@@ -755,6 +819,9 @@ def main():
                     help="3/2: the reference's default rule on the same workload (fused padded "
                          "passes); the line then times pass --timed-pass of that schedule")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-nlbatch", action="store_true")
+    ap.add_argument("--nlb-steps", type=int, default=200)
+    ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-padded", action="store_true")
     ap.add_argument("--no-cufft", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")

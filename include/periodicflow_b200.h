@@ -219,6 +219,39 @@ int pf_batch_capture(pf_batch* b, int nsteps);
 int pf_batch_replay(pf_batch* b);
 int pf_batch_sync(pf_batch* b);
 
+/* ---- realisations of one configuration in one launch ---------------------
+ * No single reference counterpart: the reference runs one realisation per
+ * mpirun (simulation.py:189-225).  pf_create_members makes one handle for
+ * `members` boxes of cfg -- nonlinear, with a fused schedule (3D 2/3 rule
+ * FP32/FP64 and 3/2 rule, 2D 2/3 rule), no injected noise -- whose states sit
+ * one after another on the device; every fused pass of a stage is one launch
+ * over all members, and each member keeps its own dt (CFL), time and forcing
+ * band energy.  Member m draws Philox noise with seed cfg->seed + m, so it
+ * equals a single solver created with that seed.  pf_step, pf_graph_capture /
+ * pf_graph_replay, pf_autotune, pf_set_linear_operator / pf_set_correlation
+ * (shared by all members), pf_project and pf_mask_zero_mode act on every
+ * member; pf_set_fourier / pf_get_fourier move all members' states as one
+ * (members, dim, spectral) array; pf_get_time and pf_energy report member 0.
+ * Physical-space transfers, pf_spectrum, pf_compute_rhs and history
+ * recording take one-member handles (PF_ERR_UNSUPPORTED otherwise). */
+int pf_create_members(const pf_config* cfg, int members, pf_solver** out);
+int pf_footprint_members(const pf_config* cfg, int members, unsigned long long* bytes);
+int pf_members(const pf_solver* h, int* members);
+int pf_set_fourier_member(pf_solver* h, int member, const double* u_hat, int where);
+int pf_get_fourier_member(pf_solver* h, int member, double* u_hat, int where);
+int pf_get_time_member(pf_solver* h, int member, double* t, double* dt);
+int pf_energy_member(pf_solver* h, int member, double* energy, double* enstrophy);
+/* Continuous batching of members (no reference counterpart): pf_step advances
+ * only members [0, active) -- the others keep their state and time -- so
+ * requests join at slot `active` and leave by moving the last active member
+ * into their slot.  Changing the count re-records the internal step graph;
+ * graphs captured with pf_graph_capture keep the count they were captured
+ * with.  pf_copy_member copies state, time and dt (device to device);
+ * pf_set_time_member sets one member's time and dt. */
+int pf_set_active_members(pf_solver* h, int active);
+int pf_copy_member(pf_solver* h, int dst, int src);
+int pf_set_time_member(pf_solver* h, int member, double t, double dt);
+
 /* ---- backward transform without device allocation ----------------------
  * No counterpart in the reference: an addition for callers that cannot call
  * cudaMalloc (a fixed memory budget handed over by an embedding application,

@@ -13,6 +13,7 @@ import glob
 import os
 import subprocess
 import sys
+import time
 from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -67,11 +68,15 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     def compile_one(item):
         src, obj = item
         cmd = [NVCC] + ARCH + FLAGS + ["-MD", "-MF", obj[:-2] + ".d", "-c", src, "-o", obj]
+        start = time.time()
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed on {src}:\n{r.stderr}")
         if verbose and r.stderr.strip():
             sys.stderr.write(r.stderr)
+        # stamp the object with the compile's start: a source or header
+        # edited while it compiled is newer, so the next build redoes it
+        os.utime(obj, (start, start))
         return obj
 
     if todo:

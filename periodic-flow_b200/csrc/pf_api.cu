@@ -17,6 +17,11 @@ struct pf_solver {
   pf_config cfg;
   Geo g;
   int d = 0, ncomp = 0, prec = 0;
+  // members: nmem boxes of this configuration advanced together, laid out one
+  // after another in uhat, u0, nl (d nspec complex each), dscal (kScalCount)
+  // and maxbits; the fused passes cover them in one launch per pass
+  int nmem = 1;
+  int nact = 1;  // members [0, nact) take part in pf_step (pf_set_active_members)
   size_t rsz = 4;  // sizeof(real)
   cudaStream_t st = nullptr;
   void* uhat = nullptr;   // d * nspec complex
@@ -364,7 +369,7 @@ static int step_generic(pf_solver* h) {
     if (h->cfg.is_nonlinear) {
       if (use_fused) {
         if (s == 0 && cfl)
-          PF_CUDA(h, cudaMemsetAsync(h->maxbits, 0, sizeof(unsigned long long), h->st));
+          PF_CUDA(h, cudaMemsetAsync(h->maxbits, 0, sizeof(unsigned long long) * h->nact, h->st));
         for (int p = 1; p <= 4; ++p) {
           tmark(h, PF_PASS_FUSED_P1 + p - 1);
           cudaError_t fe = fused_pass(h->fused, p, h->uhat, h->nl,
@@ -376,13 +381,15 @@ static int step_generic(pf_solver* h) {
         PF_CUDA(h, h->padded ? nonlinear_padded<R>(h, s == 0 && cfl)
                              : nonlinear_generic<R>(h, s == 0 && cfl));
       }
-      if (s == 0 && cfl) PF_CUDA(h, launch_set_dt(h->dscal, h->maxbits, h->cfg.cfl, h->st));
+      if (s == 0 && cfl)
+        PF_CUDA(h, launch_set_dt(h->dscal, h->maxbits, h->cfg.cfl, h->st, h->nact));
     } else if (s == 0 && cfl) {
       return fail(h, PF_ERR_UNSUPPORTED, "CFL-adaptive dt needs the nonlinear term");
     }
     if (forcing)
       PF_CUDA(h, launch_band_energy<R>((const cx<R>*)h->uhat, g,
-                                       h->cfg.forcing_kf * h->cfg.forcing_kf, h->dscal, h->st));
+                                       h->cfg.forcing_kf * h->cfg.forcing_kf, h->dscal, h->st,
+                                       h->nact));
     UpdateArgs<R> A;
     memset(&A, 0, sizeof(A));
     A.uhat = (cx<R>*)h->uhat;
@@ -407,6 +414,7 @@ static int step_generic(pf_solver* h) {
     A.save_u0 = s == 0;
     A.nyq_mask = h->cfg.mask_nyquist;
     A.forcing = forcing;
+    A.mstride = (long long)h->d * g.nspec;
     cudaError_t ue;
     if (use_fused) {
       tmark(h, PF_PASS_FUSED_P5);
@@ -419,7 +427,7 @@ static int step_generic(pf_solver* h) {
     }
     PF_CUDA(h, ue);
   }
-  if (!cfl) PF_CUDA(h, launch_advance_time(h->dscal, 1, h->st));
+  if (!cfl) PF_CUDA(h, launch_advance_time(h->dscal, 1, h->st, h->nact));
   return PF_OK;
 }
 
@@ -619,16 +627,25 @@ static int validate(const pf_config* c) {
   return PF_OK;
 }
 
-int pf_create(const pf_config* cfg, pf_solver** out) {
+static int create_impl(const pf_config* cfg, int nmem, pf_solver** out) {
   if (!cfg || !out) return fail(nullptr, PF_ERR_INVALID, "pf_create: null argument");
   *out = nullptr;
   int rc = validate(cfg);
   if (rc) return rc;
+  if (nmem < 1) return fail(nullptr, PF_ERR_INVALID, "pf_create_members: members must be >= 1");
+  if (nmem > 1 && (!cfg->is_nonlinear || !cfg->fused))
+    return fail(nullptr, PF_ERR_UNSUPPORTED,
+                "pf_create_members: members advance through the fused nonlinear passes "
+                "(linear ensembles: pf_batch_create)");
+  if (nmem > 1 && cfg->noise_mag != 0.0 && cfg->noise_source == PF_NOISE_SRC_INJECTED)
+    return fail(nullptr, PF_ERR_UNSUPPORTED, "pf_create_members: injected noise is per solver");
   cudaError_t ce = ensure_tables();
   if (ce != cudaSuccess)
     return fail(nullptr, PF_ERR_CUDA, std::string("twiddle tables: ") + cudaGetErrorString(ce));
   pf_solver* h = new pf_solver();
   h->cfg = *cfg;
+  h->nmem = nmem;
+  h->nact = nmem;
   h->d = cfg->dim;
   h->prec = cfg->precision;
   h->rsz = h->prec == PF_FP64 ? 8 : 4;
@@ -656,11 +673,12 @@ int pf_create(const pf_config* cfg, pf_solver** out) {
   const int wc = h->d == 3 ? 3 : 1;
   h->stage64_elems = std::max((size_t)(2 * h->d * g.nspec), (size_t)(h->d * g.nphys));
   h->stage64_elems = std::max(h->stage64_elems, (size_t)(4 * h->ncomp * g.nspec));
-  bool ok = alloc(&h->uhat, cb * h->d * g.nspec) && alloc(&h->u0, cb * h->d * g.nspec) &&
+  const size_t M = (size_t)nmem;
+  bool ok = alloc(&h->uhat, cb * h->d * g.nspec * M) && alloc(&h->u0, cb * h->d * g.nspec * M) &&
             alloc(&h->spec_tmp, cb * 3 * g.nspec) &&
             alloc((void**)&h->stage64, sizeof(double) * h->stage64_elems) &&
-            alloc((void**)&h->dscal, sizeof(double) * kScalCount) &&
-            alloc((void**)&h->maxbits, sizeof(unsigned long long)) &&
+            alloc((void**)&h->dscal, sizeof(double) * kScalCount * M) &&
+            alloc((void**)&h->maxbits, sizeof(unsigned long long) * M) &&
             alloc((void**)&h->hist_dev, sizeof(double) * 2 * kHist);
   if (ok && cfg->is_nonlinear && cfg->dealias == PF_DEALIAS_PAD) {
     h->padded = true;
@@ -679,7 +697,7 @@ int pf_create(const pf_config* cfg, pf_solver** out) {
          alloc(&h->physM_u, h->rsz * h->d * gM.nphys) &&
          alloc(&h->physM_w, h->rsz * wc * gM.nphys);
   } else if (ok && cfg->is_nonlinear) {
-    ok = alloc(&h->nl, cb * h->d * g.nspec) && alloc(&h->phys_u, h->rsz * h->d * g.nphys) &&
+    ok = alloc(&h->nl, cb * h->d * g.nspec * M) && alloc(&h->phys_u, h->rsz * h->d * g.nphys) &&
          alloc(&h->phys_w, h->rsz * wc * g.nphys);
   }
   if (ok && cfg->noise_mag != 0.0 && cfg->noise_source == PF_NOISE_SRC_INJECTED)
@@ -690,12 +708,68 @@ int pf_create(const pf_config* cfg, pf_solver** out) {
     return fail(nullptr, PF_ERR_NOMEM, m);
   }
   double dt0 = cfg->dt;
-  cudaMemcpy(h->dscal + kScalDt, &dt0, sizeof(double), cudaMemcpyHostToDevice);
+  for (int m = 0; m < nmem; ++m)
+    cudaMemcpy(h->dscal + (size_t)m * kScalCount + kScalDt, &dt0, sizeof(double),
+               cudaMemcpyHostToDevice);
   if (cfg->is_nonlinear && cfg->fused) {
-    h->fused = fused_create(g, h->prec, cfg->dealias);  // nullptr when no fused path fits
+    h->fused = fused_create(g, h->prec, cfg->dealias, nmem);  // nullptr when no fused path fits
+  }
+  if (nmem > 1 && !h->fused) {
+    pf_destroy(h);
+    return fail(nullptr, PF_ERR_UNSUPPORTED,
+                "pf_create_members: no fused schedule for this geometry, precision and rule");
   }
   if (const char* v = getenv("PF_STEP_GRAPH")) h->auto_graph = atoi(v) != 0;  // 0: plain launches
   *out = h;
+  return PF_OK;
+}
+
+int pf_create(const pf_config* cfg, pf_solver** out) { return create_impl(cfg, 1, out); }
+
+int pf_create_members(const pf_config* cfg, int members, pf_solver** out) {
+  return create_impl(cfg, members, out);
+}
+
+int pf_members(const pf_solver* h, int* members) {
+  if (!h || !members) return fail(nullptr, PF_ERR_INVALID, "pf_members: null argument");
+  *members = h->nmem;
+  return PF_OK;
+}
+
+int pf_set_active_members(pf_solver* h, int active) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  if (active < 1 || active > h->nmem)
+    return fail(h, PF_ERR_INVALID, "pf_set_active_members: active must be in [1, members]");
+  if (h->capturing) return fail(h, PF_ERR_INVALID, "pf_set_active_members: inside a capture");
+  if (active == h->nact) return PF_OK;
+  h->nact = active;
+  if (h->fused) fused_set_members(h->fused, active);
+  drop_auto_graph(h);  // the recorded launches cover the old count
+  return PF_OK;
+}
+
+int pf_copy_member(pf_solver* h, int dst, int src) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  if (dst < 0 || dst >= h->nmem || src < 0 || src >= h->nmem)
+    return fail(h, PF_ERR_INVALID, "pf_copy_member: bad member");
+  if (dst == src) return PF_OK;
+  const size_t sb = 2 * h->rsz * (size_t)h->d * h->g.nspec;  // bytes of one member's state
+  PF_CUDA(h, cudaMemcpyAsync((char*)h->uhat + dst * sb, (const char*)h->uhat + src * sb, sb,
+                             cudaMemcpyDeviceToDevice, h->st));
+  PF_CUDA(h, cudaMemcpyAsync(h->dscal + (size_t)dst * kScalCount, h->dscal + (size_t)src * kScalCount,
+                             sizeof(double) * kScalCount, cudaMemcpyDeviceToDevice, h->st));
+  PF_CUDA(h, cudaStreamSynchronize(h->st));
+  return PF_OK;
+}
+
+int pf_set_time_member(pf_solver* h, int m, double t, double dt) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  if (m < 0 || m >= h->nmem) return fail(h, PF_ERR_INVALID, "pf_set_time_member: bad member");
+  if (!(dt > 0.0)) return fail(h, PF_ERR_INVALID, "pf_set_time_member: dt must be positive");
+  double* d = h->dscal + (size_t)m * kScalCount;
+  PF_CUDA(h, cudaMemcpyAsync(d + kScalTime, &t, sizeof(double), cudaMemcpyHostToDevice, h->st));
+  PF_CUDA(h, cudaMemcpyAsync(d + kScalDt, &dt, sizeof(double), cudaMemcpyHostToDevice, h->st));
+  PF_CUDA(h, cudaStreamSynchronize(h->st));
   return PF_OK;
 }
 
@@ -755,26 +829,57 @@ static cudaError_t convert_out(pf_solver* h, const void* src, size_t n) {
   return launched();
 }
 
+// state of member m (d nspec complex values) from / to complex128 data
+static int set_member(pf_solver* h, int m, const double* u_hat, int where) {
+  const size_t n = 2 * (size_t)h->d * h->g.nspec;  // doubles
+  int rc = stage_in(h, u_hat, n, where);
+  if (rc) return rc;
+  PF_CUDA(h, convert_in(h, (char*)h->uhat + (size_t)m * n * h->rsz, n));
+  PF_CUDA(h, cudaStreamSynchronize(h->st));
+  return PF_OK;
+}
+static int get_member(pf_solver* h, int m, double* u_hat, int where) {
+  const size_t n = 2 * (size_t)h->d * h->g.nspec;
+  PF_CUDA(h, convert_out(h, (const char*)h->uhat + (size_t)m * n * h->rsz, n));
+  return stage_out(h, u_hat, n, where);
+}
+
 int pf_set_fourier(pf_solver* h, const double* u_hat, int where) {
   if (!h || !u_hat) return fail(h, PF_ERR_INVALID, "pf_set_fourier: null argument");
   const size_t n = 2 * (size_t)h->d * h->g.nspec;
-  int rc = stage_in(h, u_hat, n, where);
-  if (rc) return rc;
-  PF_CUDA(h, convert_in(h, h->uhat, n));
-  PF_CUDA(h, cudaStreamSynchronize(h->st));
+  for (int m = 0; m < h->nmem; ++m) {
+    int rc = set_member(h, m, u_hat + (size_t)m * n, where);
+    if (rc) return rc;
+  }
   return PF_OK;
 }
 
 int pf_get_fourier(pf_solver* h, double* u_hat, int where) {
   if (!h || !u_hat) return fail(h, PF_ERR_INVALID, "pf_get_fourier: null argument");
   const size_t n = 2 * (size_t)h->d * h->g.nspec;
-  PF_CUDA(h, convert_out(h, h->uhat, n));
-  int rc = stage_out(h, u_hat, n, where);
+  for (int m = 0; m < h->nmem; ++m) {
+    int rc = get_member(h, m, u_hat + (size_t)m * n, where);
+    if (rc) return rc;
+  }
+  return check_dev_errors(h);
+}
+
+int pf_set_fourier_member(pf_solver* h, int m, const double* u_hat, int where) {
+  if (!h || !u_hat) return fail(h, PF_ERR_INVALID, "pf_set_fourier_member: null argument");
+  if (m < 0 || m >= h->nmem) return fail(h, PF_ERR_INVALID, "pf_set_fourier_member: bad member");
+  return set_member(h, m, u_hat, where);
+}
+
+int pf_get_fourier_member(pf_solver* h, int m, double* u_hat, int where) {
+  if (!h || !u_hat) return fail(h, PF_ERR_INVALID, "pf_get_fourier_member: null argument");
+  if (m < 0 || m >= h->nmem) return fail(h, PF_ERR_INVALID, "pf_get_fourier_member: bad member");
+  int rc = get_member(h, m, u_hat, where);
   return rc ? rc : check_dev_errors(h);
 }
 
 int pf_set_physical(pf_solver* h, const double* u, int where) {
   if (!h || !u) return fail(h, PF_ERR_INVALID, "pf_set_physical: null argument");
+  if (h->nmem > 1) return fail(h, PF_ERR_UNSUPPORTED, "pf_set_physical: one member at a time (pf_get_fourier_member)");
   const size_t n = (size_t)h->d * h->g.nphys;
   void* phys = h->phys_u;
   void* own = nullptr;
@@ -797,6 +902,7 @@ int pf_set_physical(pf_solver* h, const double* u, int where) {
 
 int pf_get_physical(pf_solver* h, double* u, int where) {
   if (!h || !u) return fail(h, PF_ERR_INVALID, "pf_get_physical: null argument");
+  if (h->nmem > 1) return fail(h, PF_ERR_UNSUPPORTED, "pf_get_physical: one member at a time (pf_get_fourier_member)");
   const size_t n = (size_t)h->d * h->g.nphys;
   void* phys = h->phys_u;
   void* own = nullptr;
@@ -821,23 +927,32 @@ int pf_get_physical(pf_solver* h, double* u, int where) {
 
 int pf_mask_zero_mode(pf_solver* h) {
   if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
-  if (h->prec == PF_FP64) k_scale_mask0<double><<<1, 32, 0, h->st>>>((double2*)h->uhat, h->g, h->d);
-  else k_scale_mask0<float><<<1, 32, 0, h->st>>>((float2*)h->uhat, h->g, h->d);
-  PF_CUDA(h, launched());
+  const size_t ms = (size_t)h->d * h->g.nspec;  // complex values per member
+  for (int m = 0; m < h->nmem; ++m) {
+    if (h->prec == PF_FP64)
+      k_scale_mask0<double><<<1, 32, 0, h->st>>>((double2*)h->uhat + m * ms, h->g, h->d);
+    else k_scale_mask0<float><<<1, 32, 0, h->st>>>((float2*)h->uhat + m * ms, h->g, h->d);
+    PF_CUDA(h, launched());
+  }
   return PF_OK;
 }
 
 int pf_project(pf_solver* h) {
   if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
   const unsigned b = blocks_for(h->g.nspec);
-  if (h->prec == PF_FP64) {
-    if (h->d == 3) k_project<double, 3><<<b, 256, 0, h->st>>>((double2*)h->uhat, h->g);
-    else k_project<double, 2><<<b, 256, 0, h->st>>>((double2*)h->uhat, h->g);
-  } else {
-    if (h->d == 3) k_project<float, 3><<<b, 256, 0, h->st>>>((float2*)h->uhat, h->g);
-    else k_project<float, 2><<<b, 256, 0, h->st>>>((float2*)h->uhat, h->g);
+  const size_t ms = (size_t)h->d * h->g.nspec;
+  for (int m = 0; m < h->nmem; ++m) {
+    if (h->prec == PF_FP64) {
+      double2* u = (double2*)h->uhat + m * ms;
+      if (h->d == 3) k_project<double, 3><<<b, 256, 0, h->st>>>(u, h->g);
+      else k_project<double, 2><<<b, 256, 0, h->st>>>(u, h->g);
+    } else {
+      float2* u = (float2*)h->uhat + m * ms;
+      if (h->d == 3) k_project<float, 3><<<b, 256, 0, h->st>>>(u, h->g);
+      else k_project<float, 2><<<b, 256, 0, h->st>>>(u, h->g);
+    }
+    PF_CUDA(h, launched());
   }
-  PF_CUDA(h, launched());
   return PF_OK;
 }
 
@@ -892,6 +1007,18 @@ int pf_step(pf_solver* h, int nsteps) {
   return h->prec == PF_FP64 ? step_impl<double>(h, nsteps) : step_impl<float>(h, nsteps);
 }
 
+int pf_get_time_member(pf_solver* h, int m, double* t, double* dt) {
+  if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  if (m < 0 || m >= h->nmem) return fail(h, PF_ERR_INVALID, "pf_get_time_member: bad member");
+  double sc[kScalCount];
+  PF_CUDA(h, cudaMemcpyAsync(sc, h->dscal + (size_t)m * kScalCount, sizeof(sc),
+                             cudaMemcpyDeviceToHost, h->st));
+  PF_CUDA(h, cudaStreamSynchronize(h->st));
+  if (t) *t = sc[kScalTime];
+  if (dt) *dt = sc[kScalDt];
+  return check_dev_errors(h);
+}
+
 int pf_get_time(pf_solver* h, double* t, long long* step, double* dt) {
   if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
   double sc[kScalCount];
@@ -905,19 +1032,27 @@ int pf_get_time(pf_solver* h, double* t, long long* step, double* dt) {
 
 int pf_set_time(pf_solver* h, double t, long long step) {
   if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
-  PF_CUDA(h, cudaMemcpyAsync(h->dscal + kScalTime, &t, sizeof(double), cudaMemcpyHostToDevice, h->st));
+  for (int m = 0; m < h->nmem; ++m)
+    PF_CUDA(h, cudaMemcpyAsync(h->dscal + (size_t)m * kScalCount + kScalTime, &t, sizeof(double),
+                               cudaMemcpyHostToDevice, h->st));
   PF_CUDA(h, cudaStreamSynchronize(h->st));
   h->step = step;
   return PF_OK;
 }
 
 int pf_energy(pf_solver* h, double* energy, double* enstrophy) {
+  return pf_energy_member(h, 0, energy, enstrophy);
+}
+
+int pf_energy_member(pf_solver* h, int m, double* energy, double* enstrophy) {
   if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
-  double* tmp = h->dscal + 4;  // slots 4, 5
+  if (m < 0 || m >= h->nmem) return fail(h, PF_ERR_INVALID, "pf_energy_member: bad member");
+  double* tmp = h->dscal + 4;  // slots 4, 5 of member 0 (scratch)
+  const size_t ms = (size_t)m * h->d * h->g.nspec;
   PF_CUDA(h, cudaMemsetAsync(tmp, 0, 2 * sizeof(double), h->st));
   cudaError_t e = h->prec == PF_FP64
-                      ? launch_energy<double>((const double2*)h->uhat, h->g, tmp, h->st)
-                      : launch_energy<float>((const float2*)h->uhat, h->g, tmp, h->st);
+                      ? launch_energy<double>((const double2*)h->uhat + ms, h->g, tmp, h->st)
+                      : launch_energy<float>((const float2*)h->uhat + ms, h->g, tmp, h->st);
   PF_CUDA(h, e);
   double r[2];
   PF_CUDA(h, cudaMemcpyAsync(r, tmp, sizeof(r), cudaMemcpyDeviceToHost, h->st));
@@ -929,6 +1064,8 @@ int pf_energy(pf_solver* h, double* energy, double* enstrophy) {
 
 int pf_record_history(pf_solver* h, int enable) {
   if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  if (enable && h->nmem > 1)
+    return fail(h, PF_ERR_UNSUPPORTED, "pf_record_history: per-member energies: pf_energy_member");
   h->record_hist = enable != 0;
   return PF_OK;
 }
@@ -947,6 +1084,7 @@ int pf_history(pf_solver* h, double* out, int max_steps, int* count) {
 
 int pf_spectrum(pf_solver* h, double* out, int nbins) {
   if (!h || !out || nbins <= 0) return fail(h, PF_ERR_INVALID, "pf_spectrum: bad argument");
+  if (h->nmem > 1) return fail(h, PF_ERR_UNSUPPORTED, "pf_spectrum: one member per solver");
   double* tmp = nullptr;
   PF_CUDA(h, cudaMalloc(&tmp, sizeof(double) * nbins));
   cudaError_t e = cudaMemsetAsync(tmp, 0, sizeof(double) * nbins, h->st);
@@ -1017,6 +1155,7 @@ extern "C" {
 
 int pf_compute_rhs(pf_solver* h, double a) {
   if (!h) return fail(nullptr, PF_ERR_INVALID, "null handle");
+  if (h->nmem > 1) return fail(h, PF_ERR_UNSUPPORTED, "pf_compute_rhs: one member per solver");
   if (h->capturing) return fail(h, PF_ERR_INVALID, "pf_compute_rhs: not inside a graph capture");
   return h->prec == PF_FP64 ? compute_rhs_impl<double>(h, a) : compute_rhs_impl<float>(h, a);
 }
@@ -1137,9 +1276,17 @@ extern "C" int pf_fused_variants(pf_solver* h, int* out) {
 }
 
 extern "C" int pf_footprint(const pf_config* c, unsigned long long* bytes) {
+  return pf_footprint_members(c, 1, bytes);
+}
+
+// Device bytes of create_impl(c, nmem): per-member buffers (state, u0, nl,
+// scalars, fused pass buffers) times nmem, shared scratch once.
+extern "C" int pf_footprint_members(const pf_config* c, int nmem, unsigned long long* bytes) {
   if (!c || !bytes) return fail(nullptr, PF_ERR_INVALID, "pf_footprint: null argument");
+  if (nmem < 1) return fail(nullptr, PF_ERR_INVALID, "pf_footprint_members: members must be >= 1");
   int rc = validate(c);
   if (rc) return rc;
+  const unsigned long long M = (unsigned long long)nmem;
   const int d = c->dim;
   long long nspec = 1, nphys = 1;
   for (int a = 0; a < d; ++a) {
@@ -1150,8 +1297,8 @@ extern "C" int pf_footprint(const pf_config* c, unsigned long long* bytes) {
   const int ncomp = c->noise_type == PF_NOISE_THERMAL ? d * d : d;
   unsigned long long st64 = std::max((unsigned long long)(2 * d * nspec), (unsigned long long)(d * nphys));
   st64 = std::max(st64, (unsigned long long)(4 * ncomp * nspec));
-  unsigned long long b = cb * d * nspec * 2 + cb * 3 * nspec + 8 * st64 + 8 * kScalCount + 8 +
-                         16 * kHist;
+  unsigned long long b = M * (cb * d * nspec * 2 + 8 * kScalCount + 8) + cb * 3 * nspec +
+                         8 * st64 + 16 * kHist;
   if (c->is_nonlinear && c->dealias == PF_DEALIAS_PAD) {
     unsigned long long msp = 1, mph = 1;
     for (int a = 0; a < d; ++a) {
@@ -1166,10 +1313,10 @@ extern "C" int pf_footprint(const pf_config* c, unsigned long long* bytes) {
     if (fz) {  // fused 3/2 schedule: pass buffers on the padded x0 (and x1) grid
       const unsigned long long t0 = 3ull * c->n[0] / 2, t1 = 3ull * c->n[1] / 2;
       const unsigned long long nh = c->n[2] / 2 + 1;
-      b += cb * (5ull * t0 * c->n[1] * nh + 6ull * t0 * t1 * nh + 3ull * t0 * t1 * nh);
+      b += M * cb * (5ull * t0 * c->n[1] * nh + 6ull * t0 * t1 * nh + 3ull * t0 * t1 * nh);
     }
   } else if (c->is_nonlinear) {
-    b += cb * d * nspec + rsz * d * nphys + rsz * (d == 3 ? 3 : 1) * nphys;
+    b += M * cb * d * nspec + rsz * d * nphys + rsz * (d == 3 ? 3 : 1) * nphys;
     bool pow2 = d == 3 && c->fused;
     const int nmax = c->precision == PF_FP32 ? 512 : 256;
     for (int a = 0; pow2 && a < 3; ++a) {
@@ -1181,12 +1328,12 @@ extern "C" int pf_footprint(const pf_config* c, unsigned long long* bytes) {
     }
     if (pow2) {
       const unsigned long long k1 = (c->n[1] - 1) / 3, k2 = (c->n[2] - 1) / 3;
-      b += cb * (5ull * c->n[0] * (2 * k1 + 1) * (k2 + 1) + 6ull * c->n[0] * c->n[1] * (k2 + 1));
+      b += M * cb * (5ull * c->n[0] * (2 * k1 + 1) * (k2 + 1) + 6ull * c->n[0] * c->n[1] * (k2 + 1));
     }
     bool f2 = d == 2 && c->fused;
     for (int a = 0; f2 && a < 2; ++a)
       f2 = c->n[a] >= 16 && c->n[a] <= 1024 && (c->n[a] & (c->n[a] - 1)) == 0;
-    if (f2) b += cb * 3ull * c->n[0] * ((c->n[1] - 1) / 3 + 1);  // 2D fused pass-1 scratch
+    if (f2) b += M * cb * 3ull * c->n[0] * ((c->n[1] - 1) / 3 + 1);  // 2D fused pass-1 scratch
   }
   if (c->noise_mag != 0.0 && c->noise_source == PF_NOISE_SRC_INJECTED) b += cb * 2 * ncomp * nspec;
   *bytes = b;

@@ -15,6 +15,10 @@ struct FGeo {
   long long nspec;
   int nlrow;                   // nl row stride along axis 0 (t1 nh)
   long long nlcomp;            // nl component stride (t0 t1 nh)
+  // Members: boxes of this geometry laid out one after another in every
+  // buffer (state 3 nspec, nl 3 nlcomp, A 5 t0 c1 c2, B 6 t0 t1 c2 complex
+  // values per member); each pass covers all of them in one launch.
+  int nmem;
 };
 
 // P3 of the 2/3 rule in FP32 with one shared-memory exchange per line FFT

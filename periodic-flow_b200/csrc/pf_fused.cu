@@ -21,15 +21,17 @@ static TuneKey tune_key(const FusedPlan* p) {
   return TuneKey(p->prec, p->pad ? 1 : 0, p->f.n0, p->f.n1, p->f.n2);
 }
 
-static FusedPlan* fused_create_2d(const Geo& g, int precision) {
+static FusedPlan* fused_create_2d(const Geo& g, int precision, int nmem) {
   if (!fused2d_side(g.n[0]) || !fused2d_side(g.n[1])) return nullptr;
   FusedPlan* p = new FusedPlan();
   p->g = g;
   p->prec = precision;
   p->dim = 2;
   p->f2 = fused2d_geo(g);
+  p->f2.nmem = nmem;
+  p->cap = nmem;
   const size_t cb = precision == 0 ? 8 : 16;
-  if (cudaMalloc(&p->A, cb * fused2d_scratch_elems(p->f2)) != cudaSuccess ||
+  if (cudaMalloc(&p->A, cb * nmem * fused2d_scratch_elems(p->f2)) != cudaSuccess ||
       cudaMalloc(&p->err, sizeof(int)) != cudaSuccess ||
       cudaMemset(p->err, 0, sizeof(int)) != cudaSuccess) {
     fused_destroy(p);
@@ -39,10 +41,11 @@ static FusedPlan* fused_create_2d(const Geo& g, int precision) {
   return p;
 }
 
-FusedPlan* fused_create(const Geo& g, int precision, int dealias) {
-  if ((precision != 0 && precision != 1) || (dealias != 0 && dealias != 1)) return nullptr;
+FusedPlan* fused_create(const Geo& g, int precision, int dealias, int nmem) {
+  if ((precision != 0 && precision != 1) || (dealias != 0 && dealias != 1) || nmem < 1)
+    return nullptr;
   // 2D: 2/3 rule, sides 2^b 16..1024, FP32 and FP64
-  if (g.dim == 2) return dealias == 0 ? fused_create_2d(g, precision) : nullptr;
+  if (g.dim == 2) return dealias == 0 ? fused_create_2d(g, precision, nmem) : nullptr;
   if (g.dim != 3) return nullptr;
   const bool pad = dealias == 1;
   // FP32 2/3 rule: sides 2^b 16..512 (the last up to 256) and 3 * 2^b
@@ -109,9 +112,16 @@ FusedPlan* fused_create(const Geo& g, int precision, int dealias) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, dev);
   const size_t cb = precision == 0 ? 8 : 16;
-  const size_t a_el = 5ull * f.t0 * f.c1 * f.c2, b_el = 6ull * f.t0 * f.t1 * f.c2;
+  f.nmem = nmem;
+  p->cap = nmem;
+  // the persistent pass counts line pairs of all members in 32-bit integers
+  if ((long long)nmem * f.t0 * f.t1 >= (1LL << 31)) {
+    delete p;
+    return nullptr;
+  }
+  const size_t a_el = 5ull * f.t0 * f.c1 * f.c2 * nmem, b_el = 6ull * f.t0 * f.t1 * f.c2 * nmem;
   if (cudaMalloc(&p->A, cb * a_el) != cudaSuccess || cudaMalloc(&p->B, cb * b_el) != cudaSuccess ||
-      (pad && cudaMalloc(&p->nlM, cb * (size_t)(3 * f.nlcomp)) != cudaSuccess) ||
+      (pad && cudaMalloc(&p->nlM, cb * (size_t)(3 * f.nlcomp) * nmem) != cudaSuccess) ||
       cudaMalloc(&p->err, sizeof(int)) != cudaSuccess ||
       cudaMemset(p->err, 0, sizeof(int)) != cudaSuccess) {
     fused_destroy(p);
@@ -119,6 +129,12 @@ FusedPlan* fused_create(const Geo& g, int precision, int dealias) {
     return nullptr;
   }
   return p;
+}
+
+void fused_set_members(FusedPlan* p, int active) {
+  if (!p || active < 1 || active > p->cap) return;
+  p->f.nmem = active;
+  p->f2.nmem = active;
 }
 
 void fused_destroy(FusedPlan* p) {

@@ -12,8 +12,12 @@ struct FusedPlan;
 // rule (FP32, FP64) and FP64 2/3 rule, sides 2^b 16..256; 2D: 2/3 rule, FP32
 // and FP64, sides 2^b 16..1024).  2D plans run passes 1 and 3 and the update;
 // passes 2 and 4 are no-ops there.
-FusedPlan* fused_create(const Geo& g, int precision, int dealias);
+// nmem > 1: buffers and launches for nmem boxes of this geometry laid out one
+// after another (state, nl and the device scalars of the caller likewise).
+FusedPlan* fused_create(const Geo& g, int precision, int dealias, int nmem = 1);
 void fused_destroy(FusedPlan* p);
+// Launches of the plan cover members [0, active) (active <= the plan's members).
+void fused_set_members(FusedPlan* p, int active);
 // Pass 1..4 of the nonlinear term of uhat (unprojected) into nl; pass 3
 // writes max(sum_i |u_i| / dx_i) as double bits into maxbits when non-null.
 cudaError_t fused_pass(FusedPlan* p, int pass, const void* uhat, void* nl,

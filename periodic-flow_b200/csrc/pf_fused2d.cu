@@ -66,6 +66,9 @@ k_q1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, F2 f, const cx<R>* __r
   const int q = blockIdx.x * T + t;  // kept column k1 in [0, c1)
   const bool active = q < f.c1;
   const int fld = blockIdx.y;        // 0: u0, 1: u1, 2: D
+  // member blockIdx.z of boxes laid out one after another
+  uh += (long long)blockIdx.z * 2 * f.nspec;
+  A += (long long)blockIdx.z * 3 * f.n0 * f.c1;
   const C* src = uh + (fld == 0 ? 0 : f.nspec);
   C v[E];
 #pragma unroll
@@ -97,6 +100,10 @@ k_q2(const cx<R>* __restrict__ A, cx<R>* __restrict__ nl, F2 f, const cx<R>* __r
   using C = cx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int j = threadIdx.x, lp = threadIdx.y;
+  // member blockIdx.y
+  A += (long long)blockIdx.y * 3 * f.n0 * f.c1;
+  nl += (long long)blockIdx.y * 2 * f.nspec;
+  if (maxbits) maxbits += blockIdx.y;
   const int pair = blockIdx.x * TN::LP + lp;
   const bool active = pair < (f.n0 >> 1);
   const int la = 2 * pair;
@@ -196,6 +203,8 @@ template <typename R, int N, int V, int NC, bool NOISE>
 __global__ void __launch_bounds__(Tune2<N, R, V>::TU * Tune2<N, R, V>::GS)
 k_q3(UpdateArgs<R> U, const cx<R>* __restrict__ nl, F2 f, const cx<R>* __restrict__ tw) {
   using TN = Tune2<N, R, V>;
+  const Member mem = member_of(U, blockIdx.y);  // member blockIdx.y
+  nl += (long long)blockIdx.y * 2 * f.nspec;
   constexpr int E = TN::ES, G = TN::GS, T = TN::TU;
   constexpr int CH0 = sizeof(R) == 8 ? 2 : 4;  // rows per thread whose state loads are in flight
   constexpr int CH = E < CH0 ? E : CH0;
@@ -217,12 +226,12 @@ k_q3(UpdateArgs<R> U, const cx<R>* __restrict__ nl, F2 f, const cx<R>* __restric
   }
   fft<N, E, -1>(v0, j, tw, smf, sync);
   fft<N, E, -1>(v1, j, tw, smf, sync);
-  const StageScalars<R> sc = stage_scalars<R>(U);
+  const StageScalars<R> sc = stage_scalars<R>(U, mem.mb);
   double accE = 0.0, accZ = 0.0;
   if (active) {
     const R k1 = (R)(f.ks1 * q);
-    cx<R>* __restrict__ uh = U.uhat;
-    const cx<R>* __restrict__ u0p = U.u0;
+    cx<R>* __restrict__ uh = U.uhat + mem.mo;
+    cx<R>* __restrict__ u0p = U.u0 + mem.mo;
     const long long ns = f.nspec;
 #pragma unroll
     for (int e0 = 0; e0 < E; e0 += CH) {
@@ -246,11 +255,12 @@ k_q3(UpdateArgs<R> U, const cx<R>* __restrict__ nl, F2 f, const cx<R>* __restric
         mk_.k[0] = k0; mk_.k[1] = k1;
         mk_.k2 = k0 * k0 + k1 * k1;
         C nv[2] = {v0[e0 + cc], v1[e0 + cc]};
-        update_core<R, 2, NC, NOISE>(U, m, mk_, nv, true, un[cc], u0v[cc], sc, accE, accZ);
+        update_core<R, 2, NC, NOISE>(U, m, mk_, nv, true, un[cc], u0v[cc], sc, accE, accZ, uh, u0p,
+                                     mem.mb);
       }
     }
   }
-  if (U.diag) block_add2(accE, accZ, U.diag);
+  if (U.diag) block_add2(accE, accZ, U.diag + 2 * mem.mb);
 }
 
 // ------------------------------------------------------------------ host side
@@ -265,6 +275,7 @@ F2 fused2d_geo(const Geo& g) {
   f.ks0 = g.kscale[0]; f.ks1 = g.kscale[1];
   f.cflw0 = g.n[0] * g.kscale[0] / (2.0 * M_PI);
   f.cflw1 = g.n[1] * g.kscale[1] / (2.0 * M_PI);
+  f.nmem = 1;
   // measured on B200 (RK3, FP32 and FP64): the halved radix is faster at
   // sides 256 and 512 (256^2 FP32 43 vs 60 us per step), slower at 1024
   f.var[0] = 0;
@@ -304,7 +315,7 @@ static cudaError_t q1_run(const F2& f, const cx<R>* uh, cx<R>* A, cudaStream_t s
   const size_t sm = colp_bytes<N, TN::T, R>();
   cudaError_t e = smem_limit(k_q1<R, N, V>, sm);
   if (e != cudaSuccess) return e;
-  const dim3 grid((unsigned)((f.c1 + TN::T - 1) / TN::T), 3);
+  const dim3 grid((unsigned)((f.c1 + TN::T - 1) / TN::T), 3, (unsigned)f.nmem);
   k_q1<R, N, V><<<grid, dim3(TN::T, TN::GS), sm, st>>>(uh, A, f, tw_base<R>() + tw_offset(N));
   return launched();
 }
@@ -317,7 +328,7 @@ static cudaError_t q2_run(const F2& f, const cx<R>* A, cx<R>* nl, unsigned long 
   cudaError_t e = smem_limit(k_q2<R, N, V>, sm);
   if (e != cudaSuccess) return e;
   const int npairs = f.n0 / 2;
-  const dim3 grid((unsigned)((npairs + TN::LP - 1) / TN::LP));
+  const dim3 grid((unsigned)((npairs + TN::LP - 1) / TN::LP), (unsigned)f.nmem);
   const R scale = (R)(1.0 / ((double)f.n0 * (double)f.n1));
   k_q2<R, N, V><<<grid, dim3(TN::GC, TN::LP), sm, st>>>(A, nl, f, tw_base<R>() + tw_offset(N),
                                                          maxbits, scale);
@@ -329,7 +340,8 @@ static cudaError_t q3_run(const F2& f, const UpdateArgs<R>& U, int ncomp, const 
                           cudaStream_t st) {
   using TN = Tune2<N, R, V>;
   const size_t sm = colp_bytes<N, TN::TU, R>();
-  const dim3 grid((unsigned)((f.nh + TN::TU - 1) / TN::TU)), block(TN::TU, TN::GS);
+  const dim3 grid((unsigned)((f.nh + TN::TU - 1) / TN::TU), (unsigned)f.nmem),
+      block(TN::TU, TN::GS);
   const cx<R>* tw = tw_base<R>() + tw_offset(N);
   cudaError_t e;
   if (U.noise_src == kNoiseNone) {

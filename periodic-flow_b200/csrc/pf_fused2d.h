@@ -13,6 +13,8 @@ struct F2 {
   double ks0, ks1;      // 2 pi / L_i
   double cflw0, cflw1;  // n_i / L_i
   int var[4];           // launch form of Q1..Q3 (0: default, 1: halved radix, sides >= 256)
+  int nmem;             // members laid out one after another (state and nl 2 nspec,
+                        // pass-1 buffer 3 n0 c1 complex values each), one launch per pass
 };
 
 // Sides with a fused 2D schedule: powers of two 16..1024 (FP32 and FP64).

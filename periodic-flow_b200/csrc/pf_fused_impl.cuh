@@ -122,6 +122,7 @@ struct FusedPlan {
   int dim = 3;        // 2: the three-pass 2D schedule of pf_fused2d.cu on f2 (A its scratch)
   F2 f2;
   int* err = nullptr; // device error word (bounded waits that gave up)
+  int cap = 1;        // members the buffers hold (f.nmem / f2.nmem: members launched)
   int nsm = 148;
   // launch variant per pass (used where that pass's axis has 256 points):
   // measured best on B200 at 256^3 are P1 one output field per CTA row
@@ -140,6 +141,15 @@ struct FusedPlan {
   bool fp64_rows = true;
 };
 
+// CFL maximum of a warp into member m's slot (double bits, atomicMax on the
+// bit pattern of a non-negative double); every lane calls it.
+PF_D void flush_max(unsigned long long* maxbits, int m, double& mx) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(maxbits + m, (unsigned long long)__double_as_longlong(mx));
+  mx = 0.0;
+}
+
 // ---------------------------------------------------------------------- P1
 template <typename R, int N, int E, int T, int MB, bool PAD, bool FIVE = false>
 __global__ void __launch_bounds__(T * (N / E), MB)
@@ -149,7 +159,10 @@ k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
   using C = cx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
-  // 32-bit offsets: every fused index space is below 2^31 for sides <= 512
+  // member blockIdx.z; 32-bit offsets inside a member: every fused index
+  // space is below 2^31 for sides <= 512
+  uh += (long long)blockIdx.z * 3 * f.nspec;
+  A += (long long)blockIdx.z * 5 * f.t0 * f.c1 * f.c2;
   const int t = threadIdx.x, j = threadIdx.y;
   const int ncols = f.c1 * f.c2;
   const int q = blockIdx.x * T + t;
@@ -245,6 +258,8 @@ k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
   using C = cx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
+  A += (long long)blockIdx.z * 5 * f.t0 * f.c1 * f.c2;  // member blockIdx.z
+  B += (long long)blockIdx.z * 6 * f.t0 * f.t1 * f.c2;
   const int t = threadIdx.x, j = threadIdx.y;
   const int ncols = f.t0 * f.c2;
   const int q = blockIdx.x * T + t;
@@ -376,11 +391,12 @@ k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
 // G lanes).  A group's six input fields are two adjacent lines each, so one
 // bulk copy per field lands a group in shared memory; the copy of the next
 // group (other stage) is in flight while the current one is transformed.
-template <typename R, int N, int NB, int W, int MB>
+// MEMB: more than one member (the member of a group is its index / gpm).
+template <typename R, int N, int NB, int W, int MB, bool MEMB = false>
 __global__ void __launch_bounds__(32 * W, MB)
 k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
      const cx<R>* __restrict__ tw, unsigned long long* __restrict__ maxbits, R scale,
-     int* __restrict__ err, long long ngroups) {
+     int* __restrict__ err, int ngroups) {
   constexpr int E = TuneC<N>::E, G = TuneC<N>::G, PW = TuneC<N>::PW;
   constexpr int H = N / 2;
   constexpr int BUF = TuneC<N>::BUF;
@@ -396,6 +412,7 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
   const int WC = ((NB * SC + PW * BUF) + 15) & ~15;
   const uint32_t fbytes = (uint32_t)(fb * sizeof(C));
   const long long fs_in = (long long)f.n0 * f.n1 * f.c2;
+  const int gpm = f.t0 * f.t1 / (2 * PW);  // groups per member
   uint64_t* bars = reinterpret_cast<uint64_t*>(smraw) + NB * warp;
   C* wbase = reinterpret_cast<C*>(smraw + 128) + (long long)warp * WC;
   C* ex = wbase + NB * SC + pw * BUF;
@@ -405,11 +422,12 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
     fence_mbar_init();
   }
   __syncwarp();
-  auto issue = [&](long long grp, int s) {
+  auto issue = [&](int grp, int s) {
     if (lane == 0) {
       fence_proxy_async_smem();
       mbar_arrive_expect_tx(&bars[s], 6 * fbytes);
-      const C* src = B + grp * fb;
+      const int mem = MEMB ? grp / gpm : 0;  // member of the group
+      const C* src = B + (long long)mem * 6 * fs_in + (long long)(grp - mem * gpm) * fb;
       C* dst = wbase + s * SC;
 #pragma unroll
       for (int fld = 0; fld < 6; ++fld) bulk_g2s(dst + fld * fb, src + fld * fs_in, fbytes, &bars[s]);
@@ -435,12 +453,18 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
       z[e] = r;
     }
   };
-  const long long TW = (long long)gridDim.x * W;
-  long long g = (long long)blockIdx.x * W + warp;
+  const int TW = gridDim.x * W;  // groups of all members: below 2^31 (checked at plan creation)
+  int g = blockIdx.x * W + warp;
   if (g < ngroups) issue(g, 0);
   double mx = 0.0;
+  int curm = -1;  // member whose CFL maximum mx holds
   const R h = R(0.5) * scale;
   for (int it = 0; g < ngroups; g += TW, ++it) {
+    const int mem = MEMB ? g / gpm : 0;
+    if (maxbits && mem != curm) {
+      if (curm >= 0) flush_max(maxbits, curm, mx);
+      curm = mem;
+    }
     const int s = NB == 2 ? (it & 1) : 0;
     const bool more = g + TW < ngroups;
     if (NB == 2 && more) {
@@ -488,14 +512,14 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
         mx = fmax(mx, fmax(sa, sb));
       }
     }
-    const long long la = 2 * (g * PW + pw);
+    const long long la = 2 * ((long long)(g - mem * gpm) * PW + pw);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
       fft<N, E, -1>(c[i], j, tw, smf, sync);
 #pragma unroll
       for (int e = 0; e < E; ++e) smf(j + G * e) = c[i][e];
       sync();
-      C* oa = nl + i * f.nspec + la * f.nh;
+      C* oa = nl + ((long long)mem * 3 + i) * f.nlcomp + la * f.nh;
       C* ob = oa + f.nh;
 #pragma unroll
       for (int e = 0; e <= E / 2; ++e) {
@@ -513,11 +537,7 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
       sync();
     }
   }
-  if (maxbits) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if (lane == 0) atomicMax(maxbits, (unsigned long long)__double_as_longlong(mx));
-  }
+  if (maxbits && curm >= 0) flush_max(maxbits, curm, mx);
 }
 
 // P3 with omega streamed: u goes to thread-private shared-memory slots after
@@ -529,11 +549,11 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
 // (the Nyquist column halved), outputs k2 <= n2/2 (the Nyquist entry plus
 // its -n2/2 partner, the conjugate).  2/3 rule: inputs k2 <= kmax2, every
 // output k2 <= n2/2.
-template <typename R, int N, int W, bool PAD>
+template <typename R, int N, int W, bool PAD, bool MEMB = false>
 __global__ void __launch_bounds__(32 * W, 1)
 k_p3s(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
         const cx<R>* __restrict__ tw, unsigned long long* __restrict__ maxbits, R scale,
-        int* __restrict__ err, long long ngroups) {
+        int* __restrict__ err, int ngroups) {
   constexpr int E = TuneC<N, R>::E, G = TuneC<N, R>::G, PW = TuneC<N, R>::PW;
   constexpr int H = N / 2;
   constexpr int BUF = TuneC<N, R>::BUF;
@@ -548,6 +568,7 @@ k_p3s(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
   const int WC = ((SC + PW * BUF + PW * 3 * N) + 15) & ~15;
   const uint32_t fbytes = (uint32_t)(fb * sizeof(C));
   const long long fs_in = (long long)f.t0 * f.t1 * f.c2;
+  const int gpm = f.t0 * f.t1 / (2 * PW);  // groups per member
   uint64_t* bar = reinterpret_cast<uint64_t*>(smraw) + warp;
   C* wbase = reinterpret_cast<C*>(smraw + 128) + (long long)warp * WC;
   C* ex = wbase + SC + pw * BUF;
@@ -557,11 +578,12 @@ k_p3s(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
     fence_mbar_init();
   }
   __syncwarp();
-  auto issue = [&](long long grp) {
+  auto issue = [&](int grp) {
     if (lane == 0) {
       fence_proxy_async_smem();
       mbar_arrive_expect_tx(bar, 6 * fbytes);
-      const C* src = B + grp * fb;
+      const int mem = MEMB ? grp / gpm : 0;  // member of the group
+      const C* src = B + (long long)mem * 6 * fs_in + (long long)(grp - mem * gpm) * fb;
 #pragma unroll
       for (int fld = 0; fld < 6; ++fld) bulk_g2s(wbase + fld * fb, src + fld * fs_in, fbytes, bar);
     }
@@ -587,12 +609,18 @@ k_p3s(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
   };
   // line a in the real parts, line b in the imaginary parts
   auto mul = [](C p, C q) { C r; r.x = p.x * q.x; r.y = p.y * q.y; return r; };
-  const long long TW = (long long)gridDim.x * W;
-  long long g = (long long)blockIdx.x * W + warp;
+  const int TW = gridDim.x * W;  // groups of all members: below 2^31 (checked at plan creation)
+  int g = blockIdx.x * W + warp;
   if (g < ngroups) issue(g);
   double mx = 0.0;
+  int curm = -1;  // member whose CFL maximum mx holds
   const R h = R(0.5) * scale;
   for (int it = 0; g < ngroups; g += TW, ++it) {
+    const int mem = MEMB ? g / gpm : 0;
+    if (maxbits && mem != curm) {
+      if (curm >= 0) flush_max(maxbits, curm, mx);
+      curm = mem;
+    }
     const bool more = g + TW < ngroups;
     const bool ok = mbar_wait_bounded(bar, (uint32_t)(it & 1));
     if (!__all_sync(0xffffffffu, ok)) {
@@ -642,14 +670,14 @@ k_p3s(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
         c[ib][e] = csub(c[ib][e], mul(ua, v[e]));
       }
     }
-    const long long la = 2 * (g * PW + pw);
+    const long long la = 2 * ((long long)(g - mem * gpm) * PW + pw);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
       fft<N, E, -1>(c[i], j, tw, smf, sync);
 #pragma unroll
       for (int e = 0; e < E; ++e) smf(j + G * e) = c[i][e];
       sync();
-      C* oa = nl + i * f.nlcomp + la * f.nh;
+      C* oa = nl + ((long long)mem * 3 + i) * f.nlcomp + la * f.nh;
       C* ob = oa + f.nh;
 #pragma unroll
       for (int e = 0; e <= E / 2; ++e) {
@@ -671,11 +699,7 @@ k_p3s(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
       sync();
     }
   }
-  if (maxbits) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if (lane == 0) atomicMax(maxbits, (unsigned long long)__double_as_longlong(mx));
-  }
+  if (maxbits && curm >= 0) flush_max(maxbits, curm, mx);
 }
 
 // ---------------------------------------------------------------------- P4
@@ -690,6 +714,7 @@ k_p4(cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
   using C = cx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
+  nl += (long long)blockIdx.y * 3 * f.nlcomp;  // member blockIdx.y
   const int t = threadIdx.x, j = threadIdx.y;
   const long long ncols = (long long)3 * f.t0 * f.nh;
   const long long q = (long long)blockIdx.x * T + t;
@@ -734,10 +759,12 @@ k_p4(cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
 // N x T buffer per component, also the FFT's exchange buffer) so the update
 // phase holds only a chunk of modes in registers; u_hat / u0 of a chunk are
 // loaded before any of its stores.
-template <typename R, int N, int NC, bool NOISE, int CHU, bool PAD>
+template <typename R, int N, int NC, bool NOISE, int CHU, bool PAD, bool MEMB = false>
 __global__ void __launch_bounds__(TuneU<N, R>::T * TuneU<N, R>::G, sizeof(R) == 8 ? 1 : 2)
 k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
   constexpr int E = TuneU<N, R>::E, G = TuneU<N, R>::G, T = TuneU<N, R>::T;
+  const Member mem = member_of(U, MEMB ? (int)blockIdx.y : 0);  // member blockIdx.y
+  if (MEMB) nl += (long long)blockIdx.y * 3 * f.nlcomp;
   constexpr int CH = E < CHU ? E : CHU;  // rows per thread whose state loads are in flight
   using C = cx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -783,13 +810,13 @@ k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restr
       return z;
     }
   };
-  const StageScalars<R> sc = stage_scalars<R>(U);
+  const StageScalars<R> sc = stage_scalars<R>(U, mem.mb);
   double accE = 0.0, accZ = 0.0;
   if (active) {
     const int i1 = q / f.nh, i2 = q - i1 * f.nh;
     const R k1 = (R)(f.ks1 * kfreq(i1, f.n1)), k2 = (R)(f.ks2 * i2);
-    cx<R>* __restrict__ uh = U.uhat;
-    const cx<R>* __restrict__ u0p = U.u0;
+    cx<R>* __restrict__ uh = U.uhat + mem.mo;
+    cx<R>* __restrict__ u0p = U.u0 + mem.mo;
     const long long ns = f.nspec;
 #pragma unroll
     for (int e0 = 0; e0 < EU; e0 += CH) {
@@ -815,11 +842,12 @@ k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restr
         C nv[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) nv[a] = nhat(a, i0);
-        update_core<R, 3, NC, NOISE>(U, m, mk_, nv, true, un[cc], u0v[cc], sc, accE, accZ);
+        update_core<R, 3, NC, NOISE>(U, m, mk_, nv, true, un[cc], u0v[cc], sc, accE, accZ, uh, u0p,
+                                     mem.mb);
       }
     }
   }
-  if (U.diag) block_add2(accE, accZ, U.diag);
+  if (U.diag) block_add2(accE, accZ, U.diag + 2 * mem.mb);
 }
 
 // ------------------------------------------------------------------ plan / launch
@@ -888,7 +916,7 @@ static cudaError_t p1_run(FusedPlan* p, const cx<R>* uh, cudaStream_t st) {
   const size_t sm = strided_smem<R, N, E, T, PAD>();
   cudaError_t e = set_smem(k_p1<R, N, E, T, MB, PAD>, sm);
   if (e != cudaSuccess) return e;
-  const dim3 grid((unsigned)((ncols + T - 1) / T), (unsigned)p->split[1]);
+  const dim3 grid((unsigned)((ncols + T - 1) / T), (unsigned)p->split[1], (unsigned)p->f.nmem);
   k_p1<R, N, E, T, MB, PAD><<<grid, dim3(T, G), sm, st>>>(uh, (cx<R>*)p->A, p->f, tw);
   return launched();
 }
@@ -901,7 +929,7 @@ static cudaError_t p2_run(FusedPlan* p, cudaStream_t st) {
   const size_t sm = strided_smem<R, N, E, T, PAD>();
   cudaError_t e = set_smem(k_p2<R, N, E, T, MB, PAD>, sm);
   if (e != cudaSuccess) return e;
-  const dim3 grid((unsigned)((ncols + T - 1) / T), (unsigned)p->split[2]);
+  const dim3 grid((unsigned)((ncols + T - 1) / T), (unsigned)p->split[2], (unsigned)p->f.nmem);
   k_p2<R, N, E, T, MB, PAD><<<grid, dim3(T, G), sm, st>>>(
       (const cx<R>*)p->A, (cx<R>*)p->B, p->f, tw);
   return launched();
@@ -915,8 +943,8 @@ static cudaError_t p4_run(FusedPlan* p, cx<R>* nl, cudaStream_t st) {
   const size_t sm = strided_smem<R, N, E, T, PAD>();
   cudaError_t e = set_smem(k_p4<R, N, E, T, MB, PAD>, sm);
   if (e != cudaSuccess) return e;
-  k_p4<R, N, E, T, MB, PAD><<<(unsigned)((ncols + T - 1) / T), dim3(T, G), sm, st>>>(
-      nl, p->f, tw);
+  const dim3 grid((unsigned)((ncols + T - 1) / T), (unsigned)p->f.nmem);
+  k_p4<R, N, E, T, MB, PAD><<<grid, dim3(T, G), sm, st>>>(nl, p->f, tw);
   return launched();
 }
 
@@ -954,7 +982,7 @@ static cudaError_t p1five_run(FusedPlan* p, const cx<R>* uh, cudaStream_t st) {
   const size_t sm = strided_smem<R, N, E, T, PAD>();
   cudaError_t e = set_smem(k_p1<R, N, E, T, MB, PAD, true>, sm);
   if (e != cudaSuccess) return e;
-  const dim3 grid((unsigned)((ncols + T - 1) / T), 5);
+  const dim3 grid((unsigned)((ncols + T - 1) / T), 5, (unsigned)p->f.nmem);
   k_p1<R, N, E, T, MB, PAD, true><<<grid, dim3(T, G), sm, st>>>(uh, (cx<R>*)p->A, p->f, tw);
   return launched();
 }
@@ -990,7 +1018,7 @@ static cudaError_t p2six_run(FusedPlan* p, cudaStream_t st) {
   const size_t sm = strided_smem<R, N, E, T, PAD>();
   cudaError_t e = set_smem(k_p2<R, N, E, T, MB, PAD, true>, sm);
   if (e != cudaSuccess) return e;
-  const dim3 grid((unsigned)((ncols + T - 1) / T), 6);
+  const dim3 grid((unsigned)((ncols + T - 1) / T), 6, (unsigned)p->f.nmem);
   k_p2<R, N, E, T, MB, PAD, true><<<grid, dim3(T, G), sm, st>>>(
       (const cx<R>*)p->A, (cx<R>*)p->B, p->f, tw);
   return launched();
@@ -1032,7 +1060,7 @@ static cudaError_t p3s_run(FusedPlan* p, cx<R>* nl, unsigned long long* maxbits,
                            cudaStream_t st) {
   using TN = TuneC<N, R>;
   const cx<R>* tw = tw_base<R>() + tw_offset(N);
-  const long long ngroups = (long long)p->f.t0 * p->f.t1 / (2 * TN::PW);
+  const long long ngroups = (long long)p->f.nmem * p->f.t0 * p->f.t1 / (2 * TN::PW);
   const int fb = 2 * TN::PW * p->f.c2;
   const int WC = ((6 * fb + TN::PW * TN::BUF + TN::PW * 3 * N) + 15) & ~15;
   const size_t sm = 128 + sizeof(cx<R>) * (size_t)W * WC;
@@ -1041,8 +1069,15 @@ static cudaError_t p3s_run(FusedPlan* p, cx<R>* nl, unsigned long long* maxbits,
   const R scale = (R)(1.0 / ((double)p->f.t0 * p->f.t1 * p->f.t2));
   long long blocks = (ngroups + W - 1) / W;
   if (blocks > (long long)p->nsm) blocks = p->nsm;
-  k_p3s<R, N, W, PAD><<<(unsigned)blocks, 32 * W, sm, st>>>(
-      (const cx<R>*)p->B, nl, p->f, tw, maxbits, scale, p->err, ngroups);
+  if (p->f.nmem > 1) {
+    e = set_smem(k_p3s<R, N, W, PAD, true>, sm);
+    if (e != cudaSuccess) return e;
+    k_p3s<R, N, W, PAD, true><<<(unsigned)blocks, 32 * W, sm, st>>>(
+        (const cx<R>*)p->B, nl, p->f, tw, maxbits, scale, p->err, (int)ngroups);
+  } else {
+    k_p3s<R, N, W, PAD><<<(unsigned)blocks, 32 * W, sm, st>>>(
+        (const cx<R>*)p->B, nl, p->f, tw, maxbits, scale, p->err, (int)ngroups);
+  }
   return launched();
 }
 
@@ -1051,7 +1086,7 @@ template <int N, int NB, int W, int MB>
 static cudaError_t p3_run(FusedPlan* p, float2* nl, unsigned long long* maxbits, cudaStream_t st) {
   using TN = TuneC<N>;
   const float2* tw = tw_base<float>() + tw_offset(N);
-  const long long ngroups = (long long)p->f.n0 * p->f.n1 / (2 * TN::PW);
+  const long long ngroups = (long long)p->f.nmem * p->f.n0 * p->f.n1 / (2 * TN::PW);
   const int fb = 2 * TN::PW * p->f.c2;
   const int WC = ((NB * 6 * fb + TN::PW * TN::BUF) + 15) & ~15;
   const size_t sm = 128 + sizeof(float2) * (size_t)W * WC;
@@ -1060,8 +1095,15 @@ static cudaError_t p3_run(FusedPlan* p, float2* nl, unsigned long long* maxbits,
   const float scale = (float)(1.0 / ((double)p->f.n0 * p->f.n1 * p->f.n2));
   long long blocks = (ngroups + W - 1) / W;
   if (blocks > (long long)p->nsm * MB) blocks = (long long)p->nsm * MB;
-  k_p3<float, N, NB, W, MB><<<(unsigned)blocks, 32 * W, sm, st>>>(
-      (const float2*)p->B, nl, p->f, tw, maxbits, scale, p->err, ngroups);
+  if (p->f.nmem > 1) {
+    e = set_smem(k_p3<float, N, NB, W, MB, true>, sm);
+    if (e != cudaSuccess) return e;
+    k_p3<float, N, NB, W, MB, true><<<(unsigned)blocks, 32 * W, sm, st>>>(
+        (const float2*)p->B, nl, p->f, tw, maxbits, scale, p->err, (int)ngroups);
+  } else {
+    k_p3<float, N, NB, W, MB><<<(unsigned)blocks, 32 * W, sm, st>>>(
+        (const float2*)p->B, nl, p->f, tw, maxbits, scale, p->err, (int)ngroups);
+  }
   return launched();
 }
 
@@ -1071,7 +1113,7 @@ static inline cudaError_t p3q_go(FusedPlan* p, int n, int W, float2* nl, unsigne
                           cudaStream_t st) {
   const float2* tw = tw_base<float>() + tw_offset(n);
   const int pw = 32 / (n / 16);
-  const long long ngroups = (long long)p->f.n0 * p->f.n1 / (2 * pw);
+  const long long ngroups = (long long)p->f.nmem * p->f.n0 * p->f.n1 / (2 * pw);
   const float scale = (float)(1.0 / ((double)p->f.n0 * p->f.n1 * p->f.n2));
   return p3q_launch(n, W, (const float2*)p->B, nl, p->f, tw, maxbits, scale, p->err, ngroups,
                     p->nsm, st);
@@ -1109,6 +1151,23 @@ static cudaError_t p3_n(FusedPlan* p, cx<R>* nl, unsigned long long* maxbits, cu
   }
 }
 
+// the single-box or the member form of P5
+template <typename R, bool PAD, int N, int CH, int NC, bool NOISE>
+static cudaError_t p5_go(FusedPlan* p, const UpdateArgs<R>& U, const cx<R>* nl, dim3 grid,
+                         dim3 block, size_t sm, const cx<R>* tw, cudaStream_t st) {
+  cudaError_t e;
+  if (p->f.nmem > 1) {
+    e = set_smem(k_p5<R, N, NC, NOISE, CH, PAD, true>, sm);
+    if (e != cudaSuccess) return e;
+    k_p5<R, N, NC, NOISE, CH, PAD, true><<<grid, block, sm, st>>>(U, nl, p->f, tw);
+  } else {
+    e = set_smem(k_p5<R, N, NC, NOISE, CH, PAD>, sm);
+    if (e != cudaSuccess) return e;
+    k_p5<R, N, NC, NOISE, CH, PAD><<<grid, block, sm, st>>>(U, nl, p->f, tw);
+  }
+  return cudaSuccess;
+}
+
 template <typename R, bool PAD, int N, int CH>
 static cudaError_t p5_run(FusedPlan* p, const UpdateArgs<R>& U, int ncomp, const cx<R>* nl,
                           cudaStream_t st) {
@@ -1116,22 +1175,13 @@ static cudaError_t p5_run(FusedPlan* p, const UpdateArgs<R>& U, int ncomp, const
   const cx<R>* tw = tw_base<R>() + tw_offset(N);
   const long long ncols = (long long)p->f.n1 * p->f.nh;
   const size_t sm = sizeof(cx<R>) * 3 * N * TN::T;
-  const dim3 grid((unsigned)((ncols + TN::T - 1) / TN::T)), block(TN::T, TN::G);
+  const dim3 grid((unsigned)((ncols + TN::T - 1) / TN::T), (unsigned)p->f.nmem),
+      block(TN::T, TN::G);
   cudaError_t e;
-  if (U.noise_src == kNoiseNone) {
-    e = set_smem(k_p5<R, N, 3, false, CH, PAD>, sm);
-    if (e != cudaSuccess) return e;
-    k_p5<R, N, 3, false, CH, PAD><<<grid, block, sm, st>>>(U, nl, p->f, tw);
-  } else if (ncomp == 9) {
-    e = set_smem(k_p5<R, N, 9, true, CH, PAD>, sm);
-    if (e != cudaSuccess) return e;
-    k_p5<R, N, 9, true, CH, PAD><<<grid, block, sm, st>>>(U, nl, p->f, tw);
-  } else {
-    e = set_smem(k_p5<R, N, 3, true, CH, PAD>, sm);
-    if (e != cudaSuccess) return e;
-    k_p5<R, N, 3, true, CH, PAD><<<grid, block, sm, st>>>(U, nl, p->f, tw);
-  }
-  return launched();
+  if (U.noise_src == kNoiseNone) e = p5_go<R, PAD, N, CH, 3, false>(p, U, nl, grid, block, sm, tw, st);
+  else if (ncomp == 9) e = p5_go<R, PAD, N, CH, 9, true>(p, U, nl, grid, block, sm, tw, st);
+  else e = p5_go<R, PAD, N, CH, 3, true>(p, U, nl, grid, block, sm, tw, st);
+  return e != cudaSuccess ? e : launched();
 }
 
 // Variant 0 keeps the state loads of 4 rows per thread in flight (FP64: 2);

@@ -27,6 +27,10 @@ template <typename R> struct UpdateArgs {
   double nu, noise_mag, noise_norm, f_eps, f_kf2;
   uint64_t seed, step;
   int noise_src, noise_type, save_u0, nyq_mask, forcing;
+  // batched boxes (member mb of a launch): state at uhat/u0 + mb * mstride,
+  // scalars at dscal + mb * kScalCount, E/Z sums at diag + 2 mb, Philox key
+  // seed + mb
+  long long mstride;
 };
 
 template <typename R> struct StokesArgs {
@@ -80,7 +84,10 @@ template <typename R>
 cudaError_t launch_curl_masked(cx<R>* dst, const cx<R>* u, const Geo& g, cudaStream_t st);
 template <typename R>
 cudaError_t launch_cross(R* u, const R* w, const Geo& g, unsigned long long* maxbits, cudaStream_t st);
-cudaError_t launch_set_dt(double* dscal, const unsigned long long* maxbits, double cfl, cudaStream_t st);
+// The per-step scalar kernels cover nmem members (dscal, maxbits, u strided
+// by kScalCount, 1 and d nspec per member).
+cudaError_t launch_set_dt(double* dscal, const unsigned long long* maxbits, double cfl, cudaStream_t st,
+                          int nmem = 1);
 // 3/2 rule: N-grid spectrum (or its curl) onto the M = 3N/2 grid, and back
 template <typename R>
 cudaError_t launch_pad(cx<R>* dst, const cx<R>* src, const Geo& gN, const Geo& gM, int ncomp,
@@ -88,10 +95,10 @@ cudaError_t launch_pad(cx<R>* dst, const cx<R>* src, const Geo& gN, const Geo& g
 template <typename R>
 cudaError_t launch_truncate(cx<R>* dst, const cx<R>* src, const Geo& gN, const Geo& gM,
                             int ncomp, cudaStream_t st);
-cudaError_t launch_advance_time(double* dscal, int n, cudaStream_t st);
+cudaError_t launch_advance_time(double* dscal, int n, cudaStream_t st, int nmem = 1);
 template <typename R>
 cudaError_t launch_band_energy(const cx<R>* u, const Geo& g, double kf2, double* dscal,
-                               cudaStream_t st);
+                               cudaStream_t st, int nmem = 1);
 template <typename R>
 cudaError_t launch_energy(const cx<R>* u, const Geo& g, double* out2, cudaStream_t st);
 template <typename R>

@@ -181,16 +181,23 @@ __global__ void k_cross(R* __restrict__ u, const R* __restrict__ w, Geo g,
   }
 }
 
-// dscal[dt] = cfl / max, from the double bits written by k_cross
-__global__ void k_set_dt(double* dscal, const unsigned long long* maxbits, double cfl) {
-  const double mx = __longlong_as_double((long long)*maxbits);
-  if (mx > 0.0) dscal[kScalDt] = cfl / mx;
-  dscal[kScalTime] += dscal[kScalDt];
+// dscal[dt] = cfl / max, from the double bits written by k_cross (one
+// thread per member)
+__global__ void k_set_dt(double* dscal, const unsigned long long* maxbits, double cfl, int nmem) {
+  for (int m = threadIdx.x; m < nmem; m += blockDim.x) {
+    double* d = dscal + (long long)m * kScalCount;
+    const double mx = __longlong_as_double((long long)maxbits[m]);
+    if (mx > 0.0) d[kScalDt] = cfl / mx;
+    d[kScalTime] += d[kScalDt];
+  }
 }
 
 // t += dt, n times (the reference accumulates t step by step, simulation.py:206)
-__global__ void k_advance_time(double* dscal, int n) {
-  for (int i = 0; i < n; ++i) dscal[kScalTime] += dscal[kScalDt];
+__global__ void k_advance_time(double* dscal, int n, int nmem) {
+  for (int m = threadIdx.x; m < nmem; m += blockDim.x) {
+    double* d = dscal + (long long)m * kScalCount;
+    for (int i = 0; i < n; ++i) d[kScalTime] += d[kScalDt];
+  }
 }
 
 // E_band = 1/2 sum_{0<|k|^2<=kf^2} w |u|^2  -> dscal[kScalBandE].  Visits only
@@ -201,6 +208,9 @@ struct BandBox { int cnt[3], K[3], full[3]; long long total; };
 template <typename R, int D>
 __global__ void k_band_energy(const cx<R>* __restrict__ u, Geo g, double kf2, BandBox bx,
                               double* dscal) {
+  // member blockIdx.y of boxes laid out one after another
+  u += (long long)blockIdx.y * D * g.nspec;
+  dscal += (long long)blockIdx.y * kScalCount;
   double acc = 0.0;
   for (long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x; b < bx.total;
        b += (long long)gridDim.x * blockDim.x) {
@@ -436,20 +446,22 @@ cudaError_t launch_cross(R* u, const R* w, const Geo& g, unsigned long long* max
 }
 
 cudaError_t launch_set_dt(double* dscal, const unsigned long long* maxbits, double cfl,
-                          cudaStream_t st) {
-  k_set_dt<<<1, 1, 0, st>>>(dscal, maxbits, cfl);
+                          cudaStream_t st, int nmem) {
+  k_set_dt<<<1, nmem < 256 ? (nmem < 32 ? 32 : nmem) : 256, 0, st>>>(dscal, maxbits, cfl, nmem);
   return launched();
 }
 
-cudaError_t launch_advance_time(double* dscal, int n, cudaStream_t st) {
-  k_advance_time<<<1, 1, 0, st>>>(dscal, n);
+cudaError_t launch_advance_time(double* dscal, int n, cudaStream_t st, int nmem) {
+  k_advance_time<<<1, nmem < 256 ? (nmem < 32 ? 32 : nmem) : 256, 0, st>>>(dscal, n, nmem);
   return launched();
 }
 
 template <typename R>
 cudaError_t launch_band_energy(const cx<R>* u, const Geo& g, double kf2, double* dscal,
-                               cudaStream_t st) {
-  cudaError_t e = cudaMemsetAsync(dscal + kScalBandE, 0, sizeof(double), st);
+                               cudaStream_t st, int nmem) {
+  // zero each member's band-energy slot (dscal rows of kScalCount doubles)
+  cudaError_t e = cudaMemset2DAsync(dscal + kScalBandE, sizeof(double) * kScalCount, 0,
+                                    sizeof(double), (size_t)nmem, st);
   if (e != cudaSuccess) return e;
   BandBox bx;
   bx.total = 1;
@@ -468,7 +480,7 @@ cudaError_t launch_band_energy(const cx<R>* u, const Geo& g, double kf2, double*
     }
     bx.total *= bx.cnt[a];
   }
-  const unsigned grid = grid_for(bx.total);
+  const dim3 grid(grid_for(bx.total), (unsigned)nmem);
   if (g.dim == 3) k_band_energy<R, 3><<<grid, kBlock, 0, st>>>(u, g, kf2, bx, dscal);
   else k_band_energy<R, 2><<<grid, kBlock, 0, st>>>(u, g, kf2, bx, dscal);
   return launched();
@@ -499,7 +511,7 @@ cudaError_t launch_spectrum(const cx<R>* u, const Geo& g, double* out, int nbins
   template cudaError_t launch_cross<R>(R*, const R*, const Geo&, unsigned long long*,       \
                                        cudaStream_t);                                       \
   template cudaError_t launch_band_energy<R>(const cx<R>*, const Geo&, double, double*,     \
-                                             cudaStream_t);                                 \
+                                             cudaStream_t, int);                            \
   template cudaError_t launch_energy<R>(const cx<R>*, const Geo&, double*, cudaStream_t);   \
   template cudaError_t launch_spectrum<R>(const cx<R>*, const Geo&, double*, int, double,   \
                                           cudaStream_t);

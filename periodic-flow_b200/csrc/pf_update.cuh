@@ -35,6 +35,21 @@ PF_D void block_add2(double a, double b, double* gl) {
   }
 }
 
+// Member mb of a launch over boxes laid out member after member: its state
+// is at uhat / u0 + mo (mo = mb * mstride), its scalars at dscal + mb *
+// kScalCount, its E/Z sums at diag + 2 mb, and it draws noise with key seed +
+// mb.  L(k) and C(k) arrays are shared.
+struct Member {
+  long long mo;
+  int mb;
+};
+template <typename R> PF_D Member member_of(const UpdateArgs<R>& A, int mb) {
+  Member r;
+  r.mb = mb;
+  r.mo = (long long)mb * A.mstride;
+  return r;
+}
+
 template <typename R, int D> struct ModeK {
   R k[D];
   R k2;
@@ -67,7 +82,7 @@ PF_D double half_weight(const Geo& g, const ModeIdx& ix) {
 // mask(k != 0) / sqrt(prod N) / sqrt(2 - 2/d) (space_solver.py:143-145, 227-238)
 template <typename R, int D, int NC>
 PF_D void load_noise(const UpdateArgs<R>& A, long long m, const ModeK<R, D>& mk_,
-                     cx<R> (&w1)[NC], cx<R> (&w2)[NC]) {
+                     cx<R> (&w1)[NC], cx<R> (&w2)[NC], int mb = 0) {
   if (A.noise_src == kNoiseInjected) {
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
@@ -79,21 +94,22 @@ PF_D void load_noise(const UpdateArgs<R>& A, long long m, const ModeK<R, D>& mk_
     const R nf = mk_.k2 == R(0) ? R(0) : (R)A.noise_norm;
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-      w1[c] = cscale(draw_value<R>(s, c, A.seed, A.step), nf);
-      w2[c] = cscale(draw_value<R>(s, NC + c, A.seed, A.step), nf);
+      w1[c] = cscale(draw_value<R>(s, c, A.seed + (uint64_t)mb, A.step), nf);
+      w2[c] = cscale(draw_value<R>(s, NC + c, A.seed + (uint64_t)mb, A.step), nf);
     }
   }
 }
 
 template <typename R> struct StageScalars { R dt, sqdt, fcoef; };
 
-template <typename R> PF_D StageScalars<R> stage_scalars(const UpdateArgs<R>& A) {
+template <typename R> PF_D StageScalars<R> stage_scalars(const UpdateArgs<R>& A, int mb = 0) {
+  const double* ds = A.dscal + (long long)mb * kScalCount;
   StageScalars<R> s;
-  s.dt = (R)A.dscal[kScalDt];
-  s.sqdt = (R)sqrt(A.dscal[kScalDt]);
+  s.dt = (R)ds[kScalDt];
+  s.sqdt = (R)sqrt(ds[kScalDt]);
   s.fcoef = R(0);
   if (A.forcing) {
-    const double ef = A.dscal[kScalBandE];
+    const double ef = ds[kScalBandE];
     s.fcoef = ef > 0.0 ? (R)(A.f_eps / (2.0 * ef)) : R(0);
   }
   return s;
@@ -102,17 +118,19 @@ template <typename R> PF_D StageScalars<R> stage_scalars(const UpdateArgs<R>& A)
 // Update of mode m from preloaded state un (current) and u0v (start of step)
 // and its unprojected nonlinear term nv (ignored when !has_nl); writes uhat
 // (and u0 at the first stage), adds to the E/Z sums.  NOISE = false compiles
-// the noise path out (noise_mag == 0).
+// the noise path out (noise_mag == 0).  The state of the mode's member is at
+// uh, u0 (A.uhat, A.u0 offset by the member), mb its member index.
 template <typename R, int D, int NC, bool NOISE>
 PF_D void update_core(const UpdateArgs<R>& A, long long m, const ModeK<R, D>& mk_,
                       cx<R> (&nv)[D], bool has_nl, cx<R> (&un)[D], const cx<R> (&u0v)[D],
-                      const StageScalars<R>& sc, double& accE, double& accZ) {
+                      const StageScalars<R>& sc, double& accE, double& accZ,
+                      cx<R>* __restrict__ uh, cx<R>* __restrict__ u0, int mb) {
   using C = cx<R>;
   const Geo& g = A.g;
   C xi[D];
   if (A.save_u0) {
 #pragma unroll
-    for (int a = 0; a < D; ++a) A.u0[a * g.nspec + m] = un[a];
+    for (int a = 0; a < D; ++a) u0[a * g.nspec + m] = un[a];
   }
   // nonlinear term: Leray projection, optional Nyquist mask (space_solver.py:297-300)
   if (has_nl) {
@@ -132,7 +150,7 @@ PF_D void update_core(const UpdateArgs<R>& A, long long m, const ModeK<R, D>& mk
   }
   if (NOISE && A.noise_src != kNoiseNone) {
     C w1[NC], w2[NC];
-    load_noise<R, D, NC>(A, m, mk_, w1, w2);
+    load_noise<R, D, NC>(A, m, mk_, w1, w2, mb);
     const R corr = A.corr ? A.corr[m] : R(0);
     noise_term<R, D, NC>(xi, w1, w2, (R)A.coef.a, A.noise_type, mk_.k, mk_.k2, corr,
                          (R)A.noise_mag);
@@ -144,7 +162,7 @@ PF_D void update_core(const UpdateArgs<R>& A, long long m, const ModeK<R, D>& mk
 #pragma unroll
   for (int a = 0; a < D; ++a) {
     const C r = stage_update<R>(A.coef, sc.dt, sc.sqdt, L, u0v[a], un[a], nv[a], xi[a]);
-    A.uhat[a * g.nspec + m] = r;
+    uh[a * g.nspec + m] = r;
     un[a] = r;
   }
   if (A.diag) {
@@ -168,7 +186,7 @@ PF_D void update_mode(const UpdateArgs<R>& A, long long m, const ModeK<R, D>& mk
     un[a] = A.uhat[a * A.g.nspec + m];
     u0v[a] = A.save_u0 ? un[a] : A.u0[a * A.g.nspec + m];
   }
-  update_core<R, D, NC, true>(A, m, mk_, nv, has_nl, un, u0v, sc, accE, accZ);
+  update_core<R, D, NC, true>(A, m, mk_, nv, has_nl, un, u0v, sc, accE, accZ, A.uhat, A.u0, 0);
 }
 
 }  // namespace pf

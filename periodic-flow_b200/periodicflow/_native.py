@@ -81,6 +81,18 @@ _SIGS = [
     ("pf_history", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     ("pf_record_history", C.c_int, [C.c_void_p, C.c_int]),
     ("pf_spectrum", C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    ("pf_create_members", C.c_int, [C.POINTER(PfConfig), C.c_int, C.POINTER(C.c_void_p)]),
+    ("pf_footprint_members", C.c_int, [C.POINTER(PfConfig), C.c_int, C.POINTER(C.c_ulonglong)]),
+    ("pf_members", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    ("pf_set_fourier_member", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    ("pf_get_fourier_member", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    ("pf_get_time_member", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double)]),
+    ("pf_energy_member", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double),
+                                   C.POINTER(C.c_double)]),
+    ("pf_set_active_members", C.c_int, [C.c_void_p, C.c_int]),
+    ("pf_copy_member", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    ("pf_set_time_member", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double]),
     ("pf_compute_rhs", C.c_int, [C.c_void_p, C.c_double]),
     ("pf_get_rhs", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
     ("pf_kernel_timer", C.c_int, [C.c_void_p, C.c_int]),

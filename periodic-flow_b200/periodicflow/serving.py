@@ -7,9 +7,11 @@ admitted requests together in rounds:
 
 * linear requests (fluctuating Stokes) go through one ensemble launch per
   round (``pf_batch_step``): all of them, of any size, in one kernel;
-* nonlinear requests (Taylor-Green) each run a chunk of steps on their own
-  CUDA stream, so their kernels overlap on the device; the ones running at
-  once stay under a cap on their total grid points (``nl_points_cap``);
+* nonlinear requests (Taylor-Green) of one grid share a pool: a
+  ``Realisations`` handle whose fused passes are one launch over every
+  request in it; pools run chunks of steps on their own CUDA streams, so
+  their kernels overlap on the device, under a cap on the grid points of the
+  chunks in flight (``nl_points_cap``);
 
 requests that finish leave at the end of the round, freeing memory and a
 slot for the next arrivals.  ``mode='serial'`` is the one-at-a-time baseline:
@@ -39,6 +41,7 @@ class Request:
     steps: int
     seed: int = 0
     admitted: float | None = None
+    started: float | None = None   # first chunk (a pool's join) or admission (linear)
     finished: float | None = None
     result: np.ndarray | None = field(default=None, repr=False)
 
@@ -76,6 +79,26 @@ def request_config(r: Request, precision="fp32"):
                         0.0, False, precision, TGV["dt"], r.seed, "philox", None, None, True)
 
 
+def tgv_spectrum(N):
+    """Normalised half spectrum of the Taylor-Green velocity (u = sin x cos y
+    cos z, v = -cos x sin y cos z, w = 0; in 2D u = sin x cos y, v = -cos x
+    sin y) on [0, 2 pi)^d: the sampled field's forward transform, which has
+    only the modes |k_i| = 1, written directly."""
+    d = len(N)
+    shape = (d,) + tuple(N[:-1]) + (N[-1] // 2 + 1,)
+    uh = np.zeros(shape, dtype=np.complex128)
+    if d == 3:
+        for s0 in (1, -1):
+            for s1 in (1, -1):
+                uh[0, s0 % N[0], s1 % N[1], 1] = -0.125j * s0
+                uh[1, s0 % N[0], s1 % N[1], 1] = 0.125j * s1
+    else:
+        for s0 in (1, -1):
+            uh[0, s0 % N[0], 1] = -0.25j * s0
+            uh[1, s0 % N[0], 1] = 0.25j
+    return uh
+
+
 def make_solver(r: Request, precision="fp32"):
     """Solver with the request's initial state (Taylor-Green velocity, or rest
     for the thermal-noise runs)."""
@@ -89,15 +112,7 @@ def make_solver(r: Request, precision="fp32"):
         return s
     s = Solver(list(r.N), TGV["dt"], 1.0, time_integrator=TGV["integrator"], viscosity=TGV["nu"],
                dealias="2/3", precision=precision)
-    x = s.space_solver.x
-    u = np.zeros((d,) + tuple(r.N))
-    if d == 3:
-        u[0] = np.sin(x[0]) * np.cos(x[1]) * np.cos(x[2])
-        u[1] = -np.cos(x[0]) * np.sin(x[1]) * np.cos(x[2])
-    else:
-        u[0] = np.sin(x[0]) * np.cos(x[1])
-        u[1] = -np.cos(x[0]) * np.sin(x[1])
-    s.initialize(u)
+    s.initialize(tgv_spectrum(r.N), "fourier")
     # the first request of each geometry tunes the fused passes' launch
     # variants; later ones start from the library's cached picks
     key = (tuple(r.N), precision)
@@ -110,10 +125,89 @@ def make_solver(r: Request, precision="fp32"):
 _TUNED: set = set()
 
 
+class Pool:
+    """Nonlinear requests of one grid advancing together: a Realisations
+    handle of `cap` slots on its own stream.  Occupied slots are [0, active);
+    a request joins at slot `active`; one that finishes leaves by moving the
+    last occupied slot into its place.  Every chunk of steps is one launch
+    sequence over all occupied slots."""
+
+    def __init__(self, N, cap, precision, torch):
+        from .ensemble import Realisations
+        self.N = tuple(N)
+        self.cap = cap
+        self.R = Realisations(self.N, TGV["dt"], cap, time_integrator=TGV["integrator"],
+                              viscosity=TGV["nu"], dealias="2/3", precision=precision)
+        key = (self.N, precision)
+        if key not in _TUNED:
+            self.R.autotune()
+            _TUNED.add(key)
+        self.stream = torch.cuda.Stream()
+        self.R.set_stream(self.stream)
+        self.event = torch.cuda.Event()
+        self.slots = []      # [request, remaining steps] of slots 0 .. active-1
+        self.waiting = []    # admitted requests joining at the next chunk boundary
+        self.chunk = 0       # steps of the chunk in flight (0: idle)
+        self.ic = tgv_spectrum(self.N)
+
+    def free(self) -> int:
+        return self.cap - len(self.slots) - len(self.waiting)
+
+    def points(self) -> int:
+        return len(self.slots) * int(np.prod(self.N))
+
+    def absorb(self):
+        """Waiting requests take the next slots (between chunks only: the
+        uploads are ordered on the pool's stream)."""
+        for r in self.waiting:
+            m = len(self.slots)
+            self.R.set_state(m, self.ic)
+            self.R.set_member_time(m, 0.0, TGV["dt"])
+            self.slots.append([r, r.steps])
+        self.waiting.clear()
+
+    def launch(self, chunk_max, now):
+        if not self.slots:
+            self.chunk = 0
+            return
+        for a in self.slots:
+            if a[0].started is None:
+                a[0].started = now
+        self.R.set_active(len(self.slots))
+        self.chunk = min(chunk_max, min(a[1] for a in self.slots))
+        self.R.step(self.chunk)
+        self.event.record(self.stream)
+
+    def collect(self, keep_results):
+        """After a chunk: the requests that finished (their results read out
+        when wanted), their slots refilled from the end."""
+        done = []
+        for a in self.slots:
+            a[1] -= self.chunk
+        m = 0
+        while m < len(self.slots):
+            if self.slots[m][1] == 0:
+                r = self.slots[m][0]
+                if keep_results:
+                    r.result = self.R.state(m)
+                done.append(r)
+                last = len(self.slots) - 1
+                if m != last:
+                    self.R.copy_member(m, last)
+                    self.slots[m] = self.slots[last]
+                self.slots.pop()
+            else:
+                m += 1
+        self.chunk = 0
+        return done
+
+
 def poisson_requests(n, rate=50.0, seed=2, min_steps=100, max_steps=5000,
-                     sizes2d=(64, 128, 256, 512, 1024), sizes3d=(32, 64, 128)):
-    """Poisson arrivals; grid sides log-uniform over the built sizes; steps
-    log-uniform in [min_steps, max_steps]; kinds and dimensions equally likely."""
+                     sizes2d=(64, 128, 256, 512, 1024), sizes3d=(32, 48, 64, 96, 128, 192)):
+    """Poisson arrivals; grid sides log-uniform over the built sizes (2D:
+    powers of two 64..1024; 3D: the ladder 32..192 of 2^b and 3 * 2^b sides,
+    ratios 1.5 and 4/3); steps log-uniform in [min_steps, max_steps]; kinds
+    and dimensions equally likely."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
@@ -129,17 +223,21 @@ def poisson_requests(n, rate=50.0, seed=2, min_steps=100, max_steps=5000,
 
 class Server:
     def __init__(self, hbm_budget=150e9, max_slots=64, chunk_nonlinear=25, chunk_linear=500,
-                 precision="fp32", keep_results=False, nl_points_cap=1 << 21):
+                 precision="fp32", keep_results=False, nl_points_cap=1 << 24,
+                 pool_points=1 << 24, max_members=64):
         self.budget = float(hbm_budget)
         self.max_slots = max_slots
-        # grid points of the nonlinear requests running at once (None: no
-        # cap).  A nonlinear request waits while the running ones and it
-        # together pass the cap (one always runs); nonlinear requests keep
-        # their arrival order, linear ones may pass a waiting one.  Nonlinear
-        # steps of grids up to 1024^2 / 128^3 work largely out of the 126 MB
-        # L2: running more of them at once evicts each other's fields (on the
-        # serving mix 2^21 points gave 1.35-1.45x the serial throughput,
-        # no cap 0.76-1.12x)
+        # a pool of nonlinear requests of one grid holds up to pool_points
+        # grid points (at most max_members requests)
+        self.pool_points = int(pool_points)
+        self.max_members = int(max_members)
+        # grid points of the nonlinear chunks in flight at once (None: no
+        # cap); a pool waits while the running ones and it together pass the
+        # cap (one always runs).  Without batching, concurrent requests of
+        # grids up to 1024^2 / 128^3 evicted each other's fields from the 126
+        # MB L2 (on the serving mix 2^21 points gave 1.35-1.45x the serial
+        # throughput, no cap 0.76-1.12x); pools stream their members through
+        # HBM in one launch, so the cap is per chunk of all members.
         self.nl_points_cap = nl_points_cap
         self.chunk_nl = chunk_nonlinear
         self.chunk_lin = chunk_linear
@@ -154,7 +252,7 @@ class Server:
         import torch
         reqs = sorted(requests, key=lambda r: r.arrival)
         for r in reqs:
-            r.admitted = r.finished = None
+            r.admitted = r.started = r.finished = None
             r.result = None
         if mode == "serial":
             return self._run_serial(reqs, torch)
@@ -171,7 +269,7 @@ class Server:
             wait = r.arrival - (time.perf_counter() - t0)
             if wait > 0:
                 time.sleep(wait)
-            r.admitted = time.perf_counter() - t0
+            r.admitted = r.started = time.perf_counter() - t0
             sol = make_solver(r, self.precision)
             sol.space_solver.step(r.steps)
             torch.cuda.synchronize()
@@ -179,19 +277,26 @@ class Server:
             del sol
         return self._metrics(reqs, "serial")
 
+    def pool_cap(self, r: Request) -> int:
+        """Slots of a new pool for r's grid: up to pool_points grid points in
+        all, at most max_members."""
+        return int(max(1, min(self.max_members, self.pool_points // r.points)))
+
     def _run_continuous(self, reqs, torch):
-        """Event-driven continuous batching: every nonlinear request advances
-        on its own stream by graph-replayed chunks and gets its next chunk as
-        soon as its previous one has completed (polled with CUDA events), so
-        small requests are not held back by large ones; all linear requests
-        advance together as one captured ensemble graph on a stream of its
-        own, re-captured at a chunk boundary when its membership changes.
-        Arrivals are admitted against the memory budget and slot limit as
-        they come."""
-        from .ensemble import Ensemble
+        """Event-driven continuous batching.  Nonlinear requests of one grid
+        share a pool (one Realisations handle on its own stream) and advance
+        together, one launch sequence per chunk over all occupied slots; a
+        request joins its pool at the next chunk boundary and leaves at the
+        one where its steps are done.  Pools run concurrently and each gets
+        its next chunk as soon as a CUDA event shows the previous one done.
+        All linear requests advance together as one captured ensemble graph on
+        a stream of its own, re-captured at a chunk boundary when its
+        membership changes.  Arrivals are admitted against the memory budget
+        (a pool counts its full capacity) and the slot limit as they come."""
+        from .ensemble import Ensemble, Realisations
         t0 = time.perf_counter()
         pending = list(reqs)
-        nl = []            # [request, solver, remaining, footprint, stream, event]
+        pools = {}         # grid -> Pool
         lin = []           # [request, solver, remaining, footprint]
         lin_wait = []      # admitted linear requests waiting for the next chunk boundary
         ens = None
@@ -200,48 +305,50 @@ class Server:
         ens_stream = torch.cuda.Stream()
         used = 0
 
+        def busy():
+            return any(p.slots or p.waiting for p in pools.values()) or lin or lin_wait
+
+        def pool_for(r):
+            nonlocal used
+            p = pools.get(r.N)
+            if p is not None:
+                return p if p.free() > 0 else None
+            cap = self.pool_cap(r)
+            fp = Realisations.footprint_of(request_config(r, self.precision), cap)
+            if used + fp > self.budget and busy():
+                return None
+            used += fp
+            p = Pool(r.N, cap, self.precision, torch)
+            pools[r.N] = p
+            return p
+
         def admit(now):
             nonlocal used
             i = 0
-            nl_blocked = False
-            nl_points = sum(a[0].points for a in nl)
-            while i < len(pending) and pending[i].arrival <= now and \
-                    len(nl) + len(lin) + len(lin_wait) < self.max_slots:
+            while i < len(pending) and pending[i].arrival <= now:
                 r = pending[i]
-                if not r.linear and self.nl_points_cap is not None and (
-                        nl_blocked or (nl and nl_points + r.points > self.nl_points_cap)):
-                    nl_blocked = True  # later nonlinear arrivals wait behind it
+                if not r.linear:
+                    p = pool_for(r)
+                    if p is None:
+                        i += 1  # pool full or no memory yet: wait
+                        continue
+                    pending.pop(i)
+                    r.admitted = time.perf_counter() - t0
+                    p.waiting.append(r)
+                    continue
+                if len(lin) + len(lin_wait) >= self.max_slots:
                     i += 1
                     continue
                 fp = self.footprint(r)
-                if used + fp > self.budget and (nl or lin or lin_wait):
+                if used + fp > self.budget and busy():
                     break  # wait for memory to free up
                 pending.pop(i)
-                if not r.linear:
-                    nl_points += r.points
-                r.admitted = time.perf_counter() - t0
-                sol = make_solver(r, self.precision)
+                r.admitted = r.started = time.perf_counter() - t0
+                lin_wait.append([r, make_solver(r, self.precision), r.steps, fp])
                 used += fp
-                if r.linear:
-                    lin_wait.append([r, sol, r.steps, fp])
-                    continue
-                stream = torch.cuda.Stream()
-                sol.space_solver.set_stream(stream)
-                torch.cuda.current_stream().synchronize()  # set-up copies done
-                if r.steps >= self.chunk_nl:
-                    sol.space_solver.capture(self.chunk_nl)
-                a = [r, sol, r.steps, fp, stream, torch.cuda.Event()]
-                launch_nl(a)
-                nl.append(a)
 
-        def launch_nl(a):
-            c = min(self.chunk_nl, a[2])
-            if c == self.chunk_nl:
-                a[1].space_solver.replay()
-            else:
-                a[1].space_solver.step(c)
-            a[2] -= c
-            a[5].record(a[4])
+        def running_points():
+            return sum(p.points() for p in pools.values() if p.chunk)
 
         def relaunch_linear():
             nonlocal ens, ens_chunk, ens_event
@@ -258,22 +365,26 @@ class Server:
             ens_event = torch.cuda.Event()
             ens_event.record(ens_stream)
 
-        while pending or nl or lin or lin_wait:
+        while pending or busy():
             admit(time.perf_counter() - t0)
             progressed = False
-            keep = []
-            for a in nl:
-                if not a[5].query():
-                    keep.append(a)
+            for p in pools.values():
+                if p.chunk and p.event.query():
+                    now = time.perf_counter() - t0
+                    for r in p.collect(self.keep_results):
+                        r.finished = now
+                    progressed = True
+            # idle pools with work start their next chunk, within the cap on
+            # the grid points of nonlinear chunks in flight (one always runs)
+            for p in pools.values():
+                if p.chunk or not (p.slots or p.waiting):
                     continue
+                p.absorb()
+                run = running_points()
+                if self.nl_points_cap is not None and run and run + p.points() > self.nl_points_cap:
+                    continue
+                p.launch(self.chunk_nl, time.perf_counter() - t0)
                 progressed = True
-                if a[2] == 0:
-                    self._finish(a[0], a[1], t0)
-                    used -= a[3]
-                else:
-                    launch_nl(a)
-                    keep.append(a)
-            nl[:] = keep
             if ens is None:
                 if lin_wait:
                     relaunch_linear()
@@ -296,7 +407,7 @@ class Server:
                     ens.replay()
                     ens_event.record(ens_stream)
             if not progressed:
-                if not (nl or lin or lin_wait) and pending:
+                if not busy() and pending:
                     time.sleep(max(0.0, pending[0].arrival - (time.perf_counter() - t0)))
                 else:
                     time.sleep(5e-5)

@@ -112,9 +112,10 @@ def test_served_results_equal_alone():
 
 
 def test_nonlinear_points_cap():
-    """With the cap at one request's points the nonlinear requests run one
-    after another in arrival order, a linear one passes them, and results
-    equal the serial run's."""
+    """With the cap at one request's points, the pool of one grid (requests 0
+    and 3, batched together) runs alone: the other grid's pool starts after
+    it is done, a linear request passes both, and results equal the serial
+    run's."""
     from periodicflow.serving import Request, Server
     reqs = [Request(0, 0.0, "tgv", (32, 32, 32), 60),
             Request(1, 0.0, "tgv", (64, 64), 60),
@@ -125,9 +126,31 @@ def test_nonlinear_points_cap():
     m = srv.run(reqs, "continuous")
     assert m["requests"] == 4
     mixed = {r.rid: r.result for r in reqs}
-    assert reqs[1].admitted >= reqs[0].finished
-    assert reqs[3].admitted >= reqs[1].finished
-    assert reqs[2].admitted < reqs[0].finished
+    assert reqs[3].started == reqs[0].started  # one pool, one chunk
+    assert reqs[1].started >= reqs[0].finished
+    assert reqs[2].started < reqs[0].finished
+    srv.run(reqs, "serial")
+    for r in reqs:
+        assert rel_l2(mixed[r.rid], r.result) < 1e-6, r
+
+
+def test_pool_join_and_leave_equal_alone():
+    """Requests of one grid arriving at different times with different step
+    counts share a pool: they join at chunk boundaries and leave as they
+    finish (the last occupied slot moves into the freed one); each result
+    equals the request solved alone."""
+    from periodicflow.serving import Request, Server
+    reqs = [Request(0, 0.000, "tgv", (32, 32, 32), 60),
+            Request(1, 0.005, "tgv", (32, 32, 32), 45),
+            Request(2, 0.010, "tgv", (32, 32, 32), 17),
+            Request(3, 0.020, "tgv", (32, 32, 32), 75),
+            Request(4, 0.020, "tgv", (64, 64), 50),
+            Request(5, 0.030, "tgv", (64, 64), 33),
+            Request(6, 0.040, "tgv", (32, 32, 32), 20)]
+    srv = Server(chunk_nonlinear=10, keep_results=True)
+    m = srv.run(reqs, "continuous")
+    assert m["requests"] == 7
+    mixed = {r.rid: r.result for r in reqs}
     srv.run(reqs, "serial")
     for r in reqs:
         assert rel_l2(mixed[r.rid], r.result) < 1e-6, r

@@ -97,3 +97,29 @@ def test_invalid_config_rejected_before_device_use():
     assert N.lib().pf_create(ctypes.byref(cfg), ctypes.byref(h)) == 3
     cfg.dealias = 7
     assert N.lib().pf_create(ctypes.byref(cfg), ctypes.byref(h)) == 1
+
+
+@pytest.mark.parametrize("dim,dealias,precision", [(3, "truncate", "fp32"), (3, "pad", "fp64"),
+                                                   (2, "truncate", "fp32")])
+def test_member_footprint_is_affine_in_members(dim, dealias, precision):
+    """pf_footprint_members: shared scratch once, per-member buffers times the
+    member count; one member equals pf_footprint (no device use)."""
+    import ctypes as C
+    import math
+    from periodicflow import _native as N
+    from periodicflow.space_solver import build_config
+    Ns = (64, 32, 64)[:dim]
+    cfg = build_config(Ns, [(0.0, 2 * math.pi)] * dim, True, N.PF_RK3, 2e-3, "thermal", 0.0,
+                       False, precision, 1e-3, 0, "philox", None, 0.5, True, dealias=dealias)
+
+    def fp(m):
+        b = C.c_ulonglong()
+        N.check(N.lib().pf_footprint_members(C.byref(cfg), m, C.byref(b)), None, "footprint")
+        return b.value
+    one = C.c_ulonglong()
+    N.check(N.lib().pf_footprint(C.byref(cfg), C.byref(one)), None, "footprint")
+    assert fp(1) == one.value
+    assert fp(3) - fp(2) == fp(2) - fp(1) > 0
+    assert fp(1) > fp(2) - fp(1)  # the shared scratch is counted once
+    with pytest.raises(ValueError):
+        fp(0)
