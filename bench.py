@@ -78,18 +78,58 @@ def _dist():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    """SM clock, power and clock-event reasons during the timed region, read
+    (never set) through NVML every 5 ms from a thread -- the timed region can
+    be a few tens of ms -- or, without the NVML bindings, from nvidia-smi
+    every 200 ms."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+               "hw_thermal_slowdown": 0x40}
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.thread = None
+        self.rows = []
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.gpu)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
 
     def start(self):
+        import threading
+        try:
+            nv, h = self._nvml_handle()
+            smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        except Exception:
+            nv = None
+        if nv is not None:
+            self.stop_flag = threading.Event()
+
+            def poll():
+                while not self.stop_flag.is_set():
+                    try:
+                        reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    except Exception:
+                        reasons = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+                    self.rows.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), smax,
+                                      nv.nvmlDeviceGetPowerUsage(h) / 1e3, reasons))
+                    time.sleep(0.005)
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
@@ -101,6 +141,17 @@ class ClockSampler:
             self.proc = None
 
     def stop(self):
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join()
+            rows = self.rows
+            if not rows:
+                return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+            reasons = sorted({k for r in rows for k, b in self.REASONS.items() if r[3] & b})
+            return {"sm_mhz": float(np.median([r[0] for r in rows])),
+                    "sm_max_mhz": float(max(r[1] for r in rows)), "reasons": reasons,
+                    "samples": len(rows), "source": "nvml, every 5 ms",
+                    "power_w_max": float(max(r[2] for r in rows))}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         time.sleep(0.25)
@@ -125,7 +176,7 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
         return {"sm_mhz": float(np.nanmedian(sm)), "sm_max_mhz": float(np.nanmax(smax)),
-                "reasons": reasons, "samples": len(rows),
+                "reasons": reasons, "samples": len(rows), "source": "nvidia-smi, every 200 ms",
                 "power_w_max": float(np.nanmax([num(r[3]) for r in rows]))}
 
 
@@ -165,9 +216,16 @@ def run_ours(args, dist, rank, world):
     ss.step(args.warmup)
     torch.cuda.synchronize()
     lib = N.lib()
-    # ------------------------------------------------------------ timed region
+    # The K timed steps are captured as one CUDA graph (outside the timed
+    # region) with the per-launch timer of the dominant pass inside it as
+    # event nodes, then replayed once: graph launches, and every launch of
+    # that pass still timed on its own stream.
+    stream = torch.cuda.Stream()
+    ss.set_stream(stream)
     dominant = N.PF_PASS_FUSED[args.timed_pass]
     N.check(lib.pf_kernel_timer(ss._h, dominant), ss._h, "timer")
+    ss.capture(args.steps)
+    # ------------------------------------------------------------ timed region
     c0 = C.c_longlong()
     lib.pf_launch_count(C.byref(c0))
     clocks = ClockSampler(dev)
@@ -176,9 +234,10 @@ def run_ours(args, dist, rank, world):
         dist.barrier()
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record()
-    ss.step(args.steps)
-    ev1.record()
+    with torch.cuda.stream(stream):
+        ev0.record()
+        ss.replay()
+        ev1.record()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -268,6 +327,7 @@ def run_ours(args, dist, rank, world):
                        "grid": [n, n, n], "integrator": "rk3", "replicas_per_gpu": 1,
                        "parallelism": f"replicas x{world} (one box per GPU)",
                        "l2": "working set > L2 (state 3x67.6 MB + intermediates)",
+                       "timed_launch": f"{args.steps} steps captured as one CUDA graph, replayed once",
                        "launch_variants": variants,
                        "autotuned": not args.no_autotune,
                        "dt_after_run": dt_now},
@@ -619,6 +679,27 @@ def run_serving(args):
     return out
 
 
+def run_case(args):
+    """One solver of the forced-turbulence configuration on a grid of side
+    args.n in args.dim dimensions (FP32, 2/3 rule, RK3, CFL 0.5, band
+    forcing, seed-1 field) advanced args.steps steps with the library's
+    default launch forms: the command profiles are captured on."""
+    import torch
+    from periodicflow import _comm, simulation as sim
+    from periodicflow.basis import FourierSpace
+    from periodicflow.initial import spectral_random_field
+    torch.cuda.set_device(0)
+    N = [args.n] * args.dim
+    s = sim.Solver(N, CFG["dt0"], 1.0, time_integrator=CFG["integrator"], viscosity=CFG["nu"],
+                   dealias="2/3", precision="fp32", forcing=CFG["forcing"], cfl=CFG["cfl"])
+    uh = spectral_random_field(FourierSpace(_comm.COMM_WORLD, 0, N, dealias="2/3"), CFG["seed"])
+    s.space_solver.initialize_velocity(uh, "fourier")
+    s.space_solver.step(args.steps)
+    torch.cuda.synchronize()
+    print(json.dumps({"mode": "case", "grid": N, "steps": args.steps,
+                      "launch_variants": s.space_solver.fused_variants()}), flush=True)
+
+
 def run_batched_nonlinear(args):
     """Realisations of a nonlinear configuration in one launch per fused pass
     (pf_create_members) against the same boxes solved one at a time through
@@ -814,7 +895,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--ref-budget-s", type=float, default=120.0)
-    ap.add_argument("--mode", choices=["headline", "ensemble", "serving"], default="headline")
+    ap.add_argument("--mode", choices=["headline", "ensemble", "serving", "case"],
+                    default="headline",
+                    help="case: run the forced-turbulence step on a --dim-dimensional "
+                         "grid of side --n for --steps steps, untimed (the case profiles "
+                         "are captured on)")
+    ap.add_argument("--dim", type=int, default=3, choices=[2, 3])
     ap.add_argument("--dealias", choices=["2/3", "3/2"], default="2/3",
                     help="3/2: the reference's default rule on the same workload (fused padded "
                          "passes); the line then times pass --timed-pass of that schedule")
@@ -838,6 +924,9 @@ def main():
                     help="cap on grid points of concurrently running nonlinear requests "
                          "(0: none; default: the server's)")
     args = ap.parse_args()
+    if args.mode == "case":
+        run_case(args)
+        return
     if args.mode in ("ensemble", "serving"):
         import torch
         torch.cuda.set_device(0)

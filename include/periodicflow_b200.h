@@ -191,7 +191,9 @@ int pf_get_rhs(pf_solver* h, int which, double* out, int where);
 #define PF_PASS_FUSED_P4 14
 #define PF_PASS_FUSED_P5 15
 /* Time every launch of `pass` with CUDA events on the handle's stream
- * (-1 disables); accumulators restart. */
+ * (-1 disables); accumulators restart.  Steps captured with pf_graph_capture
+ * while the timer is on carry its events as graph nodes: read the timer after
+ * one replay (a further replay records the same events again). */
 int pf_kernel_timer(pf_solver* h, int pass);
 /* Sum of the timed launch durations (ms) and their count since the last read. */
 int pf_kernel_timer_read(pf_solver* h, double* total_ms, long long* launches);

@@ -79,15 +79,18 @@ static void drop_auto_graph(pf_solver* h) {
 }
 
 // record an event on the solver stream when `pass` is the timed pass; events
-// come in (begin, end) pairs around each launch of that pass
+// come in (begin, end) pairs around each launch of that pass.  Inside a
+// pf_graph_capture the records become event nodes of the graph (external
+// records), so a replay of the captured steps times every launch in it.
 static void tmark(pf_solver* h, int pass) {
-  if (h->tpass != pass || h->capturing) return;
+  if (h->tpass != pass) return;
   if (h->tused == h->tev.size()) {
     cudaEvent_t e;
     if (cudaEventCreate(&e) != cudaSuccess) return;
     h->tev.push_back(e);
   }
-  cudaEventRecord(h->tev[h->tused++], h->st);
+  if (h->capturing) cudaEventRecordWithFlags(h->tev[h->tused++], h->st, cudaEventRecordExternal);
+  else cudaEventRecord(h->tev[h->tused++], h->st);
 }
 
 static const int kHist = 4096;

@@ -91,6 +91,7 @@ FusedPlan* fused_create(const Geo& g, int precision, int dealias, int nmem) {
       }
     }
   }
+
   if (const char* v = getenv("PF_FUSED_VARIANT")) {
     // "p1:1,p2:2,p4:1"
     for (const char* c = v; *c; ++c)
@@ -114,11 +115,6 @@ FusedPlan* fused_create(const Geo& g, int precision, int dealias, int nmem) {
   const size_t cb = precision == 0 ? 8 : 16;
   f.nmem = nmem;
   p->cap = nmem;
-  // the persistent pass counts line pairs of all members in 32-bit integers
-  if ((long long)nmem * f.t0 * f.t1 >= (1LL << 31)) {
-    delete p;
-    return nullptr;
-  }
   const size_t a_el = 5ull * f.t0 * f.c1 * f.c2 * nmem, b_el = 6ull * f.t0 * f.t1 * f.c2 * nmem;
   if (cudaMalloc(&p->A, cb * a_el) != cudaSuccess || cudaMalloc(&p->B, cb * b_el) != cudaSuccess ||
       (pad && cudaMalloc(&p->nlM, cb * (size_t)(3 * f.nlcomp) * nmem) != cudaSuccess) ||
@@ -204,11 +200,12 @@ static std::vector<int> candidates(const FusedPlan* p, int pass, bool& is384) {
     if (!p->pad && f.n2 == 128) c = {0, 4};
     return c;
   }
+  if (f.nmem > 1) return c;  // members use one launch form for passes 1, 2 and 4
   const int len = pass == 1 ? f.t0 : f.t1;
   if (len == 256) {
     c = {0, 1, 2, 3, 4, 5, 6};
-    if (pass == 2) c.insert(c.end(), {7, 8});
-    if (pass == 1) c.push_back(7);
+    if (pass == 2) c.insert(c.end(), {7, 8, 9});
+    if (pass == 1) c.insert(c.end(), {7, 9});
   } else if (len == 384) {
     is384 = true;
     c = {0, 11, 12, 13, 14, 15, 16};

@@ -54,7 +54,7 @@ template <int N, int T, typename R> constexpr size_t colp_bytes() {
 }
 
 // ---------------------------------------------------------------------- Q1
-template <typename R, int N, int V>
+template <typename R, int N, int V, bool MEMB = false>
 __global__ void __launch_bounds__(Tune2<N, R, V>::T * Tune2<N, R, V>::GS)
 k_q1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, F2 f, const cx<R>* __restrict__ tw) {
   using TN = Tune2<N, R, V>;
@@ -66,9 +66,10 @@ k_q1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, F2 f, const cx<R>* __r
   const int q = blockIdx.x * T + t;  // kept column k1 in [0, c1)
   const bool active = q < f.c1;
   const int fld = blockIdx.y;        // 0: u0, 1: u1, 2: D
-  // member blockIdx.z of boxes laid out one after another
-  uh += (long long)blockIdx.z * 2 * f.nspec;
-  A += (long long)blockIdx.z * 3 * f.n0 * f.c1;
+  if constexpr (MEMB) {  // member blockIdx.z of boxes laid out one after another
+    uh += (long long)blockIdx.z * 2 * f.nspec;
+    A += (long long)blockIdx.z * 3 * f.n0 * f.c1;
+  }
   const C* src = uh + (fld == 0 ? 0 : f.nspec);
   C v[E];
 #pragma unroll
@@ -90,7 +91,7 @@ k_q1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, F2 f, const cx<R>* __r
 }
 
 // ---------------------------------------------------------------------- Q2
-template <typename R, int N, int V>
+template <typename R, int N, int V, bool MEMB = false>
 __global__ void __launch_bounds__(Tune2<N, R, V>::GC * Tune2<N, R, V>::LP)
 k_q2(const cx<R>* __restrict__ A, cx<R>* __restrict__ nl, F2 f, const cx<R>* __restrict__ tw,
      unsigned long long* __restrict__ maxbits, R scale) {
@@ -100,10 +101,11 @@ k_q2(const cx<R>* __restrict__ A, cx<R>* __restrict__ nl, F2 f, const cx<R>* __r
   using C = cx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int j = threadIdx.x, lp = threadIdx.y;
-  // member blockIdx.y
-  A += (long long)blockIdx.y * 3 * f.n0 * f.c1;
-  nl += (long long)blockIdx.y * 2 * f.nspec;
-  if (maxbits) maxbits += blockIdx.y;
+  if constexpr (MEMB) {  // member blockIdx.y
+    A += (long long)blockIdx.y * 3 * f.n0 * f.c1;
+    nl += (long long)blockIdx.y * 2 * f.nspec;
+    if (maxbits) maxbits += blockIdx.y;
+  }
   const int pair = blockIdx.x * TN::LP + lp;
   const bool active = pair < (f.n0 >> 1);
   const int la = 2 * pair;
@@ -199,12 +201,12 @@ k_q2(const cx<R>* __restrict__ A, cx<R>* __restrict__ nl, F2 f, const cx<R>* __r
 }
 
 // ---------------------------------------------------------------------- Q3
-template <typename R, int N, int V, int NC, bool NOISE>
+template <typename R, int N, int V, int NC, bool NOISE, bool MEMB = false>
 __global__ void __launch_bounds__(Tune2<N, R, V>::TU * Tune2<N, R, V>::GS)
 k_q3(UpdateArgs<R> U, const cx<R>* __restrict__ nl, F2 f, const cx<R>* __restrict__ tw) {
   using TN = Tune2<N, R, V>;
-  const Member mem = member_of(U, blockIdx.y);  // member blockIdx.y
-  nl += (long long)blockIdx.y * 2 * f.nspec;
+  const Member mem = member_of(U, MEMB ? (int)blockIdx.y : 0);  // member blockIdx.y
+  if constexpr (MEMB) nl += (long long)blockIdx.y * 2 * f.nspec;
   constexpr int E = TN::ES, G = TN::GS, T = TN::TU;
   constexpr int CH0 = sizeof(R) == 8 ? 2 : 4;  // rows per thread whose state loads are in flight
   constexpr int CH = E < CH0 ? E : CH0;
@@ -313,10 +315,18 @@ template <typename R, int N, int V>
 static cudaError_t q1_run(const F2& f, const cx<R>* uh, cx<R>* A, cudaStream_t st) {
   using TN = Tune2<N, R, V>;
   const size_t sm = colp_bytes<N, TN::T, R>();
-  cudaError_t e = smem_limit(k_q1<R, N, V>, sm);
-  if (e != cudaSuccess) return e;
   const dim3 grid((unsigned)((f.c1 + TN::T - 1) / TN::T), 3, (unsigned)f.nmem);
-  k_q1<R, N, V><<<grid, dim3(TN::T, TN::GS), sm, st>>>(uh, A, f, tw_base<R>() + tw_offset(N));
+  const cx<R>* tw = tw_base<R>() + tw_offset(N);
+  cudaError_t e;
+  if (f.nmem > 1) {
+    e = smem_limit(k_q1<R, N, V, true>, sm);
+    if (e != cudaSuccess) return e;
+    k_q1<R, N, V, true><<<grid, dim3(TN::T, TN::GS), sm, st>>>(uh, A, f, tw);
+  } else {
+    e = smem_limit(k_q1<R, N, V>, sm);
+    if (e != cudaSuccess) return e;
+    k_q1<R, N, V><<<grid, dim3(TN::T, TN::GS), sm, st>>>(uh, A, f, tw);
+  }
   return launched();
 }
 
@@ -325,14 +335,38 @@ static cudaError_t q2_run(const F2& f, const cx<R>* A, cx<R>* nl, unsigned long 
                           cudaStream_t st) {
   using TN = Tune2<N, R, V>;
   const size_t sm = sizeof(cx<R>) * (size_t)TN::LP * TN::BUF;
-  cudaError_t e = smem_limit(k_q2<R, N, V>, sm);
-  if (e != cudaSuccess) return e;
   const int npairs = f.n0 / 2;
   const dim3 grid((unsigned)((npairs + TN::LP - 1) / TN::LP), (unsigned)f.nmem);
   const R scale = (R)(1.0 / ((double)f.n0 * (double)f.n1));
-  k_q2<R, N, V><<<grid, dim3(TN::GC, TN::LP), sm, st>>>(A, nl, f, tw_base<R>() + tw_offset(N),
-                                                         maxbits, scale);
+  const cx<R>* tw = tw_base<R>() + tw_offset(N);
+  cudaError_t e;
+  if (f.nmem > 1) {
+    e = smem_limit(k_q2<R, N, V, true>, sm);
+    if (e != cudaSuccess) return e;
+    k_q2<R, N, V, true><<<grid, dim3(TN::GC, TN::LP), sm, st>>>(A, nl, f, tw, maxbits, scale);
+  } else {
+    e = smem_limit(k_q2<R, N, V>, sm);
+    if (e != cudaSuccess) return e;
+    k_q2<R, N, V><<<grid, dim3(TN::GC, TN::LP), sm, st>>>(A, nl, f, tw, maxbits, scale);
+  }
   return launched();
+}
+
+// the single-box or the member form of Q3
+template <typename R, int N, int V, int NC, bool NOISE>
+static cudaError_t q3_go(const F2& f, const UpdateArgs<R>& U, const cx<R>* nl, dim3 grid,
+                         dim3 block, size_t sm, const cx<R>* tw, cudaStream_t st) {
+  cudaError_t e;
+  if (f.nmem > 1) {
+    e = smem_limit(k_q3<R, N, V, NC, NOISE, true>, sm);
+    if (e != cudaSuccess) return e;
+    k_q3<R, N, V, NC, NOISE, true><<<grid, block, sm, st>>>(U, nl, f, tw);
+  } else {
+    e = smem_limit(k_q3<R, N, V, NC, NOISE>, sm);
+    if (e != cudaSuccess) return e;
+    k_q3<R, N, V, NC, NOISE><<<grid, block, sm, st>>>(U, nl, f, tw);
+  }
+  return cudaSuccess;
 }
 
 template <typename R, int N, int V>
@@ -344,20 +378,10 @@ static cudaError_t q3_run(const F2& f, const UpdateArgs<R>& U, int ncomp, const 
       block(TN::TU, TN::GS);
   const cx<R>* tw = tw_base<R>() + tw_offset(N);
   cudaError_t e;
-  if (U.noise_src == kNoiseNone) {
-    e = smem_limit(k_q3<R, N, V, 2, false>, sm);
-    if (e != cudaSuccess) return e;
-    k_q3<R, N, V, 2, false><<<grid, block, sm, st>>>(U, nl, f, tw);
-  } else if (ncomp == 4) {
-    e = smem_limit(k_q3<R, N, V, 4, true>, sm);
-    if (e != cudaSuccess) return e;
-    k_q3<R, N, V, 4, true><<<grid, block, sm, st>>>(U, nl, f, tw);
-  } else {
-    e = smem_limit(k_q3<R, N, V, 2, true>, sm);
-    if (e != cudaSuccess) return e;
-    k_q3<R, N, V, 2, true><<<grid, block, sm, st>>>(U, nl, f, tw);
-  }
-  return launched();
+  if (U.noise_src == kNoiseNone) e = q3_go<R, N, V, 2, false>(f, U, nl, grid, block, sm, tw, st);
+  else if (ncomp == 4) e = q3_go<R, N, V, 4, true>(f, U, nl, grid, block, sm, tw, st);
+  else e = q3_go<R, N, V, 2, true>(f, U, nl, grid, block, sm, tw, st);
+  return e != cudaSuccess ? e : launched();
 }
 
 // Variant v of a pass at side N: the halved-radix form exists for N >= 256.

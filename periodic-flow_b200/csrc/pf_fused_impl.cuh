@@ -143,7 +143,7 @@ struct FusedPlan {
 
 // CFL maximum of a warp into member m's slot (double bits, atomicMax on the
 // bit pattern of a non-negative double); every lane calls it.
-PF_D void flush_max(unsigned long long* maxbits, int m, double& mx) {
+PF_D void flush_max(unsigned long long* maxbits, long long m, double& mx) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   if ((threadIdx.x & 31) == 0) atomicMax(maxbits + m, (unsigned long long)__double_as_longlong(mx));
@@ -151,7 +151,7 @@ PF_D void flush_max(unsigned long long* maxbits, int m, double& mx) {
 }
 
 // ---------------------------------------------------------------------- P1
-template <typename R, int N, int E, int T, int MB, bool PAD, bool FIVE = false>
+template <typename R, int N, int E, int T, int MB, bool PAD, bool FIVE = false, bool MEMB = false>
 __global__ void __launch_bounds__(T * (N / E), MB)
 k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
      const cx<R>* __restrict__ tw) {
@@ -159,10 +159,12 @@ k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
   using C = cx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
-  // member blockIdx.z; 32-bit offsets inside a member: every fused index
-  // space is below 2^31 for sides <= 512
-  uh += (long long)blockIdx.z * 3 * f.nspec;
-  A += (long long)blockIdx.z * 5 * f.t0 * f.c1 * f.c2;
+  // 32-bit offsets inside a box: every fused index space is below 2^31 for
+  // sides <= 512; MEMB: member blockIdx.z
+  if constexpr (MEMB) {
+    uh += (long long)blockIdx.z * 3 * f.nspec;
+    A += (long long)blockIdx.z * 5 * f.t0 * f.c1 * f.c2;
+  }
   const int t = threadIdx.x, j = threadIdx.y;
   const int ncols = f.c1 * f.c2;
   const int q = blockIdx.x * T + t;
@@ -250,7 +252,7 @@ k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
 }
 
 // ---------------------------------------------------------------------- P2
-template <typename R, int N, int E, int T, int MB, bool PAD, bool SIX = false>
+template <typename R, int N, int E, int T, int MB, bool PAD, bool SIX = false, bool MEMB = false>
 __global__ void __launch_bounds__(T * (N / E), MB)
 k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
      const cx<R>* __restrict__ tw) {
@@ -258,8 +260,10 @@ k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
   using C = cx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
-  A += (long long)blockIdx.z * 5 * f.t0 * f.c1 * f.c2;  // member blockIdx.z
-  B += (long long)blockIdx.z * 6 * f.t0 * f.t1 * f.c2;
+  if constexpr (MEMB) {  // member blockIdx.z
+    A += (long long)blockIdx.z * 5 * f.t0 * f.c1 * f.c2;
+    B += (long long)blockIdx.z * 6 * f.t0 * f.t1 * f.c2;
+  }
   const int t = threadIdx.x, j = threadIdx.y;
   const int ncols = f.t0 * f.c2;
   const int q = blockIdx.x * T + t;
@@ -396,7 +400,7 @@ template <typename R, int N, int NB, int W, int MB, bool MEMB = false>
 __global__ void __launch_bounds__(32 * W, MB)
 k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
      const cx<R>* __restrict__ tw, unsigned long long* __restrict__ maxbits, R scale,
-     int* __restrict__ err, int ngroups) {
+     int* __restrict__ err, long long ngroups) {
   constexpr int E = TuneC<N>::E, G = TuneC<N>::G, PW = TuneC<N>::PW;
   constexpr int H = N / 2;
   constexpr int BUF = TuneC<N>::BUF;
@@ -412,7 +416,7 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
   const int WC = ((NB * SC + PW * BUF) + 15) & ~15;
   const uint32_t fbytes = (uint32_t)(fb * sizeof(C));
   const long long fs_in = (long long)f.n0 * f.n1 * f.c2;
-  const int gpm = f.t0 * f.t1 / (2 * PW);  // groups per member
+  const long long gpm = (long long)f.t0 * f.t1 / (2 * PW);  // groups per member (MEMB)
   uint64_t* bars = reinterpret_cast<uint64_t*>(smraw) + NB * warp;
   C* wbase = reinterpret_cast<C*>(smraw + 128) + (long long)warp * WC;
   C* ex = wbase + NB * SC + pw * BUF;
@@ -422,12 +426,15 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
     fence_mbar_init();
   }
   __syncwarp();
-  auto issue = [&](int grp, int s) {
+  auto issue = [&](long long grp, int s) {
     if (lane == 0) {
       fence_proxy_async_smem();
       mbar_arrive_expect_tx(&bars[s], 6 * fbytes);
-      const int mem = MEMB ? grp / gpm : 0;  // member of the group
-      const C* src = B + (long long)mem * 6 * fs_in + (long long)(grp - mem * gpm) * fb;
+      const C* src = B + grp * fb;
+      if constexpr (MEMB) {  // member mem's fields start at mem * 6 * fs_in
+        const long long mem = grp / gpm;
+        src = B + mem * 6 * fs_in + (grp - mem * gpm) * fb;
+      }
       C* dst = wbase + s * SC;
 #pragma unroll
       for (int fld = 0; fld < 6; ++fld) bulk_g2s(dst + fld * fb, src + fld * fs_in, fbytes, &bars[s]);
@@ -453,17 +460,20 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
       z[e] = r;
     }
   };
-  const int TW = gridDim.x * W;  // groups of all members: below 2^31 (checked at plan creation)
-  int g = blockIdx.x * W + warp;
+  const long long TW = (long long)gridDim.x * W;
+  long long g = (long long)blockIdx.x * W + warp;
   if (g < ngroups) issue(g, 0);
   double mx = 0.0;
-  int curm = -1;  // member whose CFL maximum mx holds
+  [[maybe_unused]] long long curm = -1;  // member whose CFL maximum mx holds (MEMB)
   const R h = R(0.5) * scale;
   for (int it = 0; g < ngroups; g += TW, ++it) {
-    const int mem = MEMB ? g / gpm : 0;
-    if (maxbits && mem != curm) {
-      if (curm >= 0) flush_max(maxbits, curm, mx);
-      curm = mem;
+    long long mem = 0;
+    if constexpr (MEMB) {
+      mem = g / gpm;
+      if (maxbits && mem != curm) {
+        if (curm >= 0) flush_max(maxbits, curm, mx);
+        curm = mem;
+      }
     }
     const int s = NB == 2 ? (it & 1) : 0;
     const bool more = g + TW < ngroups;
@@ -512,14 +522,15 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
         mx = fmax(mx, fmax(sa, sb));
       }
     }
-    const long long la = 2 * ((long long)(g - mem * gpm) * PW + pw);
+    const long long la = 2 * ((g - mem * gpm) * PW + pw);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
       fft<N, E, -1>(c[i], j, tw, smf, sync);
 #pragma unroll
       for (int e = 0; e < E; ++e) smf(j + G * e) = c[i][e];
       sync();
-      C* oa = nl + ((long long)mem * 3 + i) * f.nlcomp + la * f.nh;
+      C* oa = nl + i * f.nspec + la * f.nh;
+      if constexpr (MEMB) oa += mem * 3 * f.nlcomp;
       C* ob = oa + f.nh;
 #pragma unroll
       for (int e = 0; e <= E / 2; ++e) {
@@ -537,7 +548,13 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
       sync();
     }
   }
-  if (maxbits && curm >= 0) flush_max(maxbits, curm, mx);
+  if constexpr (MEMB) {
+    if (maxbits && curm >= 0) flush_max(maxbits, curm, mx);
+  } else if (maxbits) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) atomicMax(maxbits, (unsigned long long)__double_as_longlong(mx));
+  }
 }
 
 // P3 with omega streamed: u goes to thread-private shared-memory slots after
@@ -553,7 +570,7 @@ template <typename R, int N, int W, bool PAD, bool MEMB = false>
 __global__ void __launch_bounds__(32 * W, 1)
 k_p3s(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
         const cx<R>* __restrict__ tw, unsigned long long* __restrict__ maxbits, R scale,
-        int* __restrict__ err, int ngroups) {
+        int* __restrict__ err, long long ngroups) {
   constexpr int E = TuneC<N, R>::E, G = TuneC<N, R>::G, PW = TuneC<N, R>::PW;
   constexpr int H = N / 2;
   constexpr int BUF = TuneC<N, R>::BUF;
@@ -568,7 +585,7 @@ k_p3s(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
   const int WC = ((SC + PW * BUF + PW * 3 * N) + 15) & ~15;
   const uint32_t fbytes = (uint32_t)(fb * sizeof(C));
   const long long fs_in = (long long)f.t0 * f.t1 * f.c2;
-  const int gpm = f.t0 * f.t1 / (2 * PW);  // groups per member
+  const long long gpm = (long long)f.t0 * f.t1 / (2 * PW);  // groups per member (MEMB)
   uint64_t* bar = reinterpret_cast<uint64_t*>(smraw) + warp;
   C* wbase = reinterpret_cast<C*>(smraw + 128) + (long long)warp * WC;
   C* ex = wbase + SC + pw * BUF;
@@ -578,12 +595,15 @@ k_p3s(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
     fence_mbar_init();
   }
   __syncwarp();
-  auto issue = [&](int grp) {
+  auto issue = [&](long long grp) {
     if (lane == 0) {
       fence_proxy_async_smem();
       mbar_arrive_expect_tx(bar, 6 * fbytes);
-      const int mem = MEMB ? grp / gpm : 0;  // member of the group
-      const C* src = B + (long long)mem * 6 * fs_in + (long long)(grp - mem * gpm) * fb;
+      const C* src = B + grp * fb;
+      if constexpr (MEMB) {  // member mem's fields start at mem * 6 * fs_in
+        const long long mem = grp / gpm;
+        src = B + mem * 6 * fs_in + (grp - mem * gpm) * fb;
+      }
 #pragma unroll
       for (int fld = 0; fld < 6; ++fld) bulk_g2s(wbase + fld * fb, src + fld * fs_in, fbytes, bar);
     }
@@ -609,17 +629,20 @@ k_p3s(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
   };
   // line a in the real parts, line b in the imaginary parts
   auto mul = [](C p, C q) { C r; r.x = p.x * q.x; r.y = p.y * q.y; return r; };
-  const int TW = gridDim.x * W;  // groups of all members: below 2^31 (checked at plan creation)
-  int g = blockIdx.x * W + warp;
+  const long long TW = (long long)gridDim.x * W;
+  long long g = (long long)blockIdx.x * W + warp;
   if (g < ngroups) issue(g);
   double mx = 0.0;
-  int curm = -1;  // member whose CFL maximum mx holds
+  [[maybe_unused]] long long curm = -1;  // member whose CFL maximum mx holds (MEMB)
   const R h = R(0.5) * scale;
   for (int it = 0; g < ngroups; g += TW, ++it) {
-    const int mem = MEMB ? g / gpm : 0;
-    if (maxbits && mem != curm) {
-      if (curm >= 0) flush_max(maxbits, curm, mx);
-      curm = mem;
+    long long mem = 0;
+    if constexpr (MEMB) {
+      mem = g / gpm;
+      if (maxbits && mem != curm) {
+        if (curm >= 0) flush_max(maxbits, curm, mx);
+        curm = mem;
+      }
     }
     const bool more = g + TW < ngroups;
     const bool ok = mbar_wait_bounded(bar, (uint32_t)(it & 1));
@@ -670,14 +693,15 @@ k_p3s(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
         c[ib][e] = csub(c[ib][e], mul(ua, v[e]));
       }
     }
-    const long long la = 2 * ((long long)(g - mem * gpm) * PW + pw);
+    const long long la = 2 * ((g - mem * gpm) * PW + pw);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
       fft<N, E, -1>(c[i], j, tw, smf, sync);
 #pragma unroll
       for (int e = 0; e < E; ++e) smf(j + G * e) = c[i][e];
       sync();
-      C* oa = nl + ((long long)mem * 3 + i) * f.nlcomp + la * f.nh;
+      C* oa = nl + i * f.nlcomp + la * f.nh;
+      if constexpr (MEMB) oa += mem * 3 * f.nlcomp;
       C* ob = oa + f.nh;
 #pragma unroll
       for (int e = 0; e <= E / 2; ++e) {
@@ -699,7 +723,13 @@ k_p3s(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
       sync();
     }
   }
-  if (maxbits && curm >= 0) flush_max(maxbits, curm, mx);
+  if constexpr (MEMB) {
+    if (maxbits && curm >= 0) flush_max(maxbits, curm, mx);
+  } else if (maxbits) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) atomicMax(maxbits, (unsigned long long)__double_as_longlong(mx));
+  }
 }
 
 // ---------------------------------------------------------------------- P4
@@ -707,14 +737,14 @@ k_p3s(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
 // k2) with plane = comp * t0 + x0.  3/2 rule: the t1 transform rows are then
 // truncated to the n1 N-grid rows (+n1/2 and -n1/2 folded into the Nyquist
 // row), written to the first n1 rows of the column.
-template <typename R, int N, int E, int T, int MB, bool PAD>
+template <typename R, int N, int E, int T, int MB, bool PAD, bool MEMB = false>
 __global__ void __launch_bounds__(T * (N / E), MB)
 k_p4(cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
   constexpr int G = N / E;
   using C = cx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* sm = reinterpret_cast<C*>(smraw);
-  nl += (long long)blockIdx.y * 3 * f.nlcomp;  // member blockIdx.y
+  if constexpr (MEMB) nl += (long long)blockIdx.y * 3 * f.nlcomp;  // member blockIdx.y
   const int t = threadIdx.x, j = threadIdx.y;
   const long long ncols = (long long)3 * f.t0 * f.nh;
   const long long q = (long long)blockIdx.x * T + t;
@@ -898,9 +928,9 @@ template <typename K> static cudaError_t set_smem(K kern, size_t bytes) {
 // Launch variants (radix width E, columns per CTA T, minimum CTAs per SM MB
 // that caps registers; 0: no cap) of the FP32 strided passes; variant 0 is
 // the TuneS default, 1..6 exist for n = 256 and 11..16 for 384, and P1 / P2
-// also have one-output-field-per-CTA-row forms (7, 8 at 256; 17..19 at 384)
-// (tuning knob
-// PF_FUSED_VARIANT="p1:v,p2:v,p3:v,p4:v", which overrides FusedPlan::var).
+// also have one-output-field-per-CTA-row forms (7..9 at 256; 17..19 at 384;
+// tuning knob PF_FUSED_VARIANT="p1:v,p2:v,p3:v,p4:v", which overrides
+// FusedPlan::var).
 // FP64 uses the TuneS defaults.  The 3/2 rule always needs the exchange
 // buffer (P4 folds through it).
 template <typename R, int N, int E, int T, bool PAD>
@@ -908,43 +938,43 @@ constexpr size_t strided_smem() {
   return (PAD || Plan<N, E>::stages() > 1) ? col_buf_bytes<N, T, R>() : 0;
 }
 
-template <typename R, bool PAD, int N, int E, int T, int MB = 0>
+template <typename R, bool PAD, int N, int E, int T, int MB = 0, bool MEMB = false>
 static cudaError_t p1_run(FusedPlan* p, const cx<R>* uh, cudaStream_t st) {
   constexpr int G = N / E;
   const cx<R>* tw = tw_base<R>() + tw_offset(N);
   const long long ncols = (long long)p->f.c1 * p->f.c2;
   const size_t sm = strided_smem<R, N, E, T, PAD>();
-  cudaError_t e = set_smem(k_p1<R, N, E, T, MB, PAD>, sm);
+  cudaError_t e = set_smem(k_p1<R, N, E, T, MB, PAD, false, MEMB>, sm);
   if (e != cudaSuccess) return e;
-  const dim3 grid((unsigned)((ncols + T - 1) / T), (unsigned)p->split[1], (unsigned)p->f.nmem);
-  k_p1<R, N, E, T, MB, PAD><<<grid, dim3(T, G), sm, st>>>(uh, (cx<R>*)p->A, p->f, tw);
+  const dim3 grid((unsigned)((ncols + T - 1) / T), (unsigned)p->split[1], MEMB ? (unsigned)p->f.nmem : 1u);
+  k_p1<R, N, E, T, MB, PAD, false, MEMB><<<grid, dim3(T, G), sm, st>>>(uh, (cx<R>*)p->A, p->f, tw);
   return launched();
 }
 
-template <typename R, bool PAD, int N, int E, int T, int MB = 0>
+template <typename R, bool PAD, int N, int E, int T, int MB = 0, bool MEMB = false>
 static cudaError_t p2_run(FusedPlan* p, cudaStream_t st) {
   constexpr int G = N / E;
   const cx<R>* tw = tw_base<R>() + tw_offset(N);
   const long long ncols = (long long)p->f.t0 * p->f.c2;
   const size_t sm = strided_smem<R, N, E, T, PAD>();
-  cudaError_t e = set_smem(k_p2<R, N, E, T, MB, PAD>, sm);
+  cudaError_t e = set_smem(k_p2<R, N, E, T, MB, PAD, false, MEMB>, sm);
   if (e != cudaSuccess) return e;
-  const dim3 grid((unsigned)((ncols + T - 1) / T), (unsigned)p->split[2], (unsigned)p->f.nmem);
-  k_p2<R, N, E, T, MB, PAD><<<grid, dim3(T, G), sm, st>>>(
+  const dim3 grid((unsigned)((ncols + T - 1) / T), (unsigned)p->split[2], MEMB ? (unsigned)p->f.nmem : 1u);
+  k_p2<R, N, E, T, MB, PAD, false, MEMB><<<grid, dim3(T, G), sm, st>>>(
       (const cx<R>*)p->A, (cx<R>*)p->B, p->f, tw);
   return launched();
 }
 
-template <typename R, bool PAD, int N, int E, int T, int MB = 0>
+template <typename R, bool PAD, int N, int E, int T, int MB = 0, bool MEMB = false>
 static cudaError_t p4_run(FusedPlan* p, cx<R>* nl, cudaStream_t st) {
   constexpr int G = N / E;
   const cx<R>* tw = tw_base<R>() + tw_offset(N);
   const long long ncols = (long long)3 * p->f.t0 * p->f.nh;
   const size_t sm = strided_smem<R, N, E, T, PAD>();
-  cudaError_t e = set_smem(k_p4<R, N, E, T, MB, PAD>, sm);
+  cudaError_t e = set_smem(k_p4<R, N, E, T, MB, PAD, MEMB>, sm);
   if (e != cudaSuccess) return e;
-  const dim3 grid((unsigned)((ncols + T - 1) / T), (unsigned)p->f.nmem);
-  k_p4<R, N, E, T, MB, PAD><<<grid, dim3(T, G), sm, st>>>(nl, p->f, tw);
+  const dim3 grid((unsigned)((ncols + T - 1) / T), MEMB ? (unsigned)p->f.nmem : 1u);
+  k_p4<R, N, E, T, MB, PAD, MEMB><<<grid, dim3(T, G), sm, st>>>(nl, p->f, tw);
   return launched();
 }
 
@@ -974,16 +1004,16 @@ static cudaError_t p4_run(FusedPlan* p, cx<R>* nl, cudaStream_t st) {
   return RUN<R, PAD, N, TuneS<N, R>::E, TuneS<N, R>::T>(__VA_ARGS__);
 
 // P1 with one output field per CTA row (five rows)
-template <typename R, bool PAD, int N, int E, int T, int MB = 0>
+template <typename R, bool PAD, int N, int E, int T, int MB = 0, bool MEMB = false>
 static cudaError_t p1five_run(FusedPlan* p, const cx<R>* uh, cudaStream_t st) {
   constexpr int G = N / E;
   const cx<R>* tw = tw_base<R>() + tw_offset(N);
   const long long ncols = (long long)p->f.c1 * p->f.c2;
   const size_t sm = strided_smem<R, N, E, T, PAD>();
-  cudaError_t e = set_smem(k_p1<R, N, E, T, MB, PAD, true>, sm);
+  cudaError_t e = set_smem(k_p1<R, N, E, T, MB, PAD, true, MEMB>, sm);
   if (e != cudaSuccess) return e;
-  const dim3 grid((unsigned)((ncols + T - 1) / T), 5, (unsigned)p->f.nmem);
-  k_p1<R, N, E, T, MB, PAD, true><<<grid, dim3(T, G), sm, st>>>(uh, (cx<R>*)p->A, p->f, tw);
+  const dim3 grid((unsigned)((ncols + T - 1) / T), 5, MEMB ? (unsigned)p->f.nmem : 1u);
+  k_p1<R, N, E, T, MB, PAD, true, MEMB><<<grid, dim3(T, G), sm, st>>>(uh, (cx<R>*)p->A, p->f, tw);
   return launched();
 }
 
@@ -991,6 +1021,15 @@ template <typename R, int N, bool PAD>
 static cudaError_t p1_n(FusedPlan* p, const cx<R>* uh, cudaStream_t st) {
   const int var = p->var[1], var384 = p->var384[1];
   (void)var; (void)var384;
+  if (p->f.nmem > 1) {
+    // members: the form a single box takes by default (one output field per
+    // CTA row for FP32 at 256 points and FP64 from 48), so a member's
+    // arithmetic is the single box's
+    using TS = TuneS<N, R>;
+    constexpr bool five = sizeof(R) == 8 ? N >= 48 : N == 256;
+    if constexpr (five) return p1five_run<R, PAD, N, TS::E, TS::T, 0, true>(p, uh, st);
+    else return p1_run<R, PAD, N, TS::E, TS::T, 0, true>(p, uh, st);
+  }
   if constexpr (sizeof(R) == 4 && N == 384) {
     switch (var384) {
       case 17: return p1five_run<R, PAD, 384, 24, 8>(p, uh, st);
@@ -1001,6 +1040,7 @@ static cudaError_t p1_n(FusedPlan* p, const cx<R>* uh, cudaStream_t st) {
   if constexpr (sizeof(R) == 4 && N == 256) {
     switch (var) {
       case 7: return p1five_run<R, PAD, 256, 16, 8>(p, uh, st);
+      case 9: return p1five_run<R, PAD, 256, 16, 16>(p, uh, st);
       default: break;
     }
   }
@@ -1010,16 +1050,16 @@ static cudaError_t p1_n(FusedPlan* p, const cx<R>* uh, cudaStream_t st) {
   PF_VARIANTS(p1_run, N, p, uh, st)
 }
 // P2 with one output field per CTA row (six rows)
-template <typename R, bool PAD, int N, int E, int T, int MB = 0>
+template <typename R, bool PAD, int N, int E, int T, int MB = 0, bool MEMB = false>
 static cudaError_t p2six_run(FusedPlan* p, cudaStream_t st) {
   constexpr int G = N / E;
   const cx<R>* tw = tw_base<R>() + tw_offset(N);
   const long long ncols = (long long)p->f.t0 * p->f.c2;
   const size_t sm = strided_smem<R, N, E, T, PAD>();
-  cudaError_t e = set_smem(k_p2<R, N, E, T, MB, PAD, true>, sm);
+  cudaError_t e = set_smem(k_p2<R, N, E, T, MB, PAD, true, MEMB>, sm);
   if (e != cudaSuccess) return e;
-  const dim3 grid((unsigned)((ncols + T - 1) / T), 6, (unsigned)p->f.nmem);
-  k_p2<R, N, E, T, MB, PAD, true><<<grid, dim3(T, G), sm, st>>>(
+  const dim3 grid((unsigned)((ncols + T - 1) / T), 6, MEMB ? (unsigned)p->f.nmem : 1u);
+  k_p2<R, N, E, T, MB, PAD, true, MEMB><<<grid, dim3(T, G), sm, st>>>(
       (const cx<R>*)p->A, (cx<R>*)p->B, p->f, tw);
   return launched();
 }
@@ -1027,6 +1067,11 @@ static cudaError_t p2six_run(FusedPlan* p, cudaStream_t st) {
 template <typename R, int N, bool PAD> static cudaError_t p2_n(FusedPlan* p, cudaStream_t st) {
   const int var = p->var[2], var384 = p->var384[2];
   (void)var; (void)var384;
+  if (p->f.nmem > 1) {  // members: the default tile (FP64 from 48 points: one field per row)
+    using TS = TuneS<N, R>;
+    if constexpr (sizeof(R) == 8 && N >= 48) return p2six_run<R, PAD, N, TS::E, TS::T, 0, true>(p, st);
+    else return p2_run<R, PAD, N, TS::E, TS::T, 0, true>(p, st);
+  }
   if constexpr (sizeof(R) == 4 && N == 384) {
     switch (var384) {
       case 17: return p2six_run<R, PAD, 384, 24, 8>(p, st);
@@ -1039,6 +1084,7 @@ template <typename R, int N, bool PAD> static cudaError_t p2_n(FusedPlan* p, cud
     switch (var) {
       case 7: return p2six_run<R, PAD, 256, 16, 8>(p, st);
       case 8: return p2six_run<R, PAD, 256, 16, 8, 4>(p, st);
+      case 9: return p2six_run<R, PAD, 256, 16, 16>(p, st);
       default: break;
     }
   }
@@ -1051,6 +1097,8 @@ template <typename R, int N, bool PAD>
 static cudaError_t p4_n(FusedPlan* p, cx<R>* nl, cudaStream_t st) {
   const int var = p->var[4], var384 = p->var384[4];
   (void)var; (void)var384;
+  if (p->f.nmem > 1)  // members: the default tile
+    return p4_run<R, PAD, N, TuneS<N, R>::E, TuneS<N, R>::T, 0, true>(p, nl, st);
   PF_VARIANTS(p4_run, N, p, nl, st)
 }
 
@@ -1073,10 +1121,10 @@ static cudaError_t p3s_run(FusedPlan* p, cx<R>* nl, unsigned long long* maxbits,
     e = set_smem(k_p3s<R, N, W, PAD, true>, sm);
     if (e != cudaSuccess) return e;
     k_p3s<R, N, W, PAD, true><<<(unsigned)blocks, 32 * W, sm, st>>>(
-        (const cx<R>*)p->B, nl, p->f, tw, maxbits, scale, p->err, (int)ngroups);
+        (const cx<R>*)p->B, nl, p->f, tw, maxbits, scale, p->err, ngroups);
   } else {
     k_p3s<R, N, W, PAD><<<(unsigned)blocks, 32 * W, sm, st>>>(
-        (const cx<R>*)p->B, nl, p->f, tw, maxbits, scale, p->err, (int)ngroups);
+        (const cx<R>*)p->B, nl, p->f, tw, maxbits, scale, p->err, ngroups);
   }
   return launched();
 }
@@ -1099,10 +1147,10 @@ static cudaError_t p3_run(FusedPlan* p, float2* nl, unsigned long long* maxbits,
     e = set_smem(k_p3<float, N, NB, W, MB, true>, sm);
     if (e != cudaSuccess) return e;
     k_p3<float, N, NB, W, MB, true><<<(unsigned)blocks, 32 * W, sm, st>>>(
-        (const float2*)p->B, nl, p->f, tw, maxbits, scale, p->err, (int)ngroups);
+        (const float2*)p->B, nl, p->f, tw, maxbits, scale, p->err, ngroups);
   } else {
     k_p3<float, N, NB, W, MB><<<(unsigned)blocks, 32 * W, sm, st>>>(
-        (const float2*)p->B, nl, p->f, tw, maxbits, scale, p->err, (int)ngroups);
+        (const float2*)p->B, nl, p->f, tw, maxbits, scale, p->err, ngroups);
   }
   return launched();
 }

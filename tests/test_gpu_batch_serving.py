@@ -167,3 +167,34 @@ def test_admission_respects_budget():
     admitted = sorted(r.admitted for r in reqs)
     finished = sorted(r.finished for r in reqs)
     assert admitted[2] >= finished[0]  # the third waited for memory
+
+
+def test_kernel_timer_inside_captured_graph():
+    """With the per-launch timer on, pf_graph_capture records its events as
+    graph nodes: one replay of the captured steps times every launch of the
+    pass (three RK3 stages per step), and the state equals plain stepping."""
+    import ctypes as C
+    import torch
+    from periodicflow import _native as N
+    from periodicflow import simulation as sim
+    import oracle as O
+    Nn = (64, 64, 64)
+    uh = O.spectral_random_field(O.Grid(Nn), 2)
+    kw = dict(time_integrator="rk3", viscosity=2e-3, dealias="2/3", precision="fp32", cfl=0.5)
+    a = sim.Solver(list(Nn), 1e-3, 1.0, **kw)
+    b = sim.Solver(list(Nn), 1e-3, 1.0, **kw)
+    a.initialize(uh, "fourier")
+    b.initialize(uh, "fourier")
+    st = torch.cuda.Stream()
+    ss = a.space_solver
+    ss.set_stream(st)
+    lib = N.lib()
+    N.check(lib.pf_kernel_timer(ss._h, N.PF_PASS_FUSED[5]), ss._h, "timer")
+    ss.capture(4)
+    ss.replay()
+    st.synchronize()
+    tot, cnt = C.c_double(), C.c_longlong()
+    N.check(lib.pf_kernel_timer_read(ss._h, C.byref(tot), C.byref(cnt)), ss._h, "timer read")
+    assert cnt.value == 12 and tot.value > 0.0
+    b.space_solver.step(4)
+    assert np.array_equal(ss.u_hat, b.space_solver.u_hat)

@@ -2,10 +2,11 @@
 advanced by one launch per fused pass must equal the same boxes solved one at
 a time.
 
-Without forcing every member is bit-identical to its single solver (the
-per-mode arithmetic and launch variants are the same); with band forcing the
-FP64 band-energy sum is accumulated with atomics in any order, so states
-agree to the last bits of that sum (relative L2 1e-6 FP32, 1e-13 FP64).
+A member runs the arithmetic of its single solver, but in separately compiled
+kernels (the member offsets are compile-time), whose multiply-add contraction
+may differ; the band-energy sum of the forcing is an FP64 atomic sum in any
+order.  Members therefore agree with their single solvers to rounding:
+relative L2 1e-6 in FP32, 1e-13 in FP64.
 """
 import numpy as np
 import pytest
@@ -66,8 +67,7 @@ def test_members_equal_single_solvers(case):
     R.project()
     R.step(steps)
     got = R.states()
-    forcing = kw.get("forcing") is not None
-    tol = 0.0 if not forcing else (1e-6 if kw["precision"] == "fp32" else 1e-13)
+    tol = 1e-6 if kw["precision"] == "fp32" else 1e-13
     for m, uh in enumerate(ics):
         ref, t, d = _single(N, dt, kw, uh, steps)
         assert np.array_equal(got[m], R.state(m))
@@ -95,7 +95,7 @@ def test_members_philox_noise_seed_per_member():
     R.step(3)
     for m, uh in enumerate(ics):
         ref, _, _ = _single(N, 1e-3, kw, uh, 3, seed=base + m)
-        assert np.array_equal(R.state(m), ref), m
+        assert rel_l2(R.state(m), ref) < 1e-6, m
 
 
 def test_members_vs_oracle():
@@ -184,8 +184,8 @@ def test_active_members_and_copy(N):
     assert R.time(3) == t3
     for m in (0, 1):
         ref, t, d = _single(N, 1e-3, kw, ics[m], 5)
-        assert np.array_equal(R.state(m), ref)
-        assert R.time(m) == (t, d)
+        assert rel_l2(R.state(m), ref) < 1e-6
+        assert abs(R.time(m)[0] - t) < 1e-6 * t
     # member 1 leaves; member 3 (parked after 2 steps) takes its slot and joins
     R.copy_member(1, 3)
     assert np.array_equal(R.state(1), parked[1]) and R.time(1) == t3
@@ -193,4 +193,4 @@ def test_active_members_and_copy(N):
     assert R.time(0) == (0.25, 2e-3)
     R.step(2)
     ref, _, _ = _single(N, 1e-3, kw, ics[3], 4)
-    assert np.array_equal(R.state(1), ref)
+    assert rel_l2(R.state(1), ref) < 1e-6

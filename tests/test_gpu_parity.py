@@ -330,7 +330,7 @@ def test_autotune_keeps_state_and_parity():
     before = a.space_solver.u_hat
     picks = a.space_solver.autotune()
     assert np.array_equal(a.space_solver.u_hat, before)
-    built = {1: range(0, 8), 2: range(0, 9), 3: range(0, 6), 4: range(0, 7)}
+    built = {1: range(0, 10), 2: range(0, 10), 3: range(0, 6), 4: range(0, 7)}
     assert all(picks["axes_256"][p] in built[p] for p in built)
     assert a.space_solver.fused_variants() == picks
     a.space_solver.step(1)
