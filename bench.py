@@ -531,6 +531,7 @@ def run_fp64(args, uh0):
         sol = make_solver(n, precision=prec)
         ss = sol.space_solver
         ss.initialize_velocity(uh0, "fourier")
+        ss.step(3)  # warm-up: first launches (module loading) and the step graph's recording
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -547,6 +548,7 @@ def run_fp64(args, uh0):
         torch.cuda.synchronize()
     a, b = states["fp32"], states["fp64"]
     out["steps"] = k
+    out["warmup_steps"] = 3
     out["fp32_rel_l2_vs_fp64"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
     return out
 

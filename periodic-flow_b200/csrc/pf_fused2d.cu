@@ -153,9 +153,10 @@ k_q2(const cx<R>* __restrict__ A, cx<R>* __restrict__ nl, F2 f, const cx<R>* __r
   if (maxbits) {
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-      const double sa = fabs((double)u0[e].x) * f.cflw0 + fabs((double)u1[e].x) * f.cflw1;
-      const double sb = fabs((double)u0[e].y) * f.cflw0 + fabs((double)u1[e].y) * f.cflw1;
-      mx = fmax(mx, fmax(sa, sb));
+      // CFL sums in the state's precision, the running maximum in FP64
+      const R sa = fabs(u0[e].x) * (R)f.cflw0 + fabs(u1[e].x) * (R)f.cflw1;
+      const R sb = fabs(u0[e].y) * (R)f.cflw0 + fabs(u1[e].y) * (R)f.cflw1;
+      mx = fmax(mx, (double)fmax(sa, sb));
     }
   }
   // line a in the real parts, line b in the imaginary parts:

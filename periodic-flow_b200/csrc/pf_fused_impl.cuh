@@ -126,9 +126,10 @@ struct FusedPlan {
   int nsm = 148;
   // launch variant per pass (used where that pass's axis has 256 points):
   // measured best on B200 at 256^3 are P1 one output field per CTA row
-  // (16, 8), P2 (16, 8) at >= 4 CTAs per SM, P3 one staging buffer, 4 warps
-  // x 3 CTAs
-  int var[6] = {0, 7, 5, 2, 0, 0};
+  // (16, 8), P2 (16, 8) at >= 4 CTAs per SM, P3 one staging buffer, 8 warps
+  // x 1 CTA (162 us against 175 us for 4 warps x 3 CTAs once the R2C split
+  // moved to warp shuffles: the 255-register budget holds the output phase)
+  int var[6] = {0, 7, 5, 3, 0, 0};
   // the same for 384-point passes (3/2 rule at n = 256), variants 11..19:
   // P1 one output field per CTA row at 24 values, P2 the same at twelve
   // values, P4 24 values
@@ -466,12 +467,21 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
   double mx = 0.0;
   [[maybe_unused]] long long curm = -1;  // member whose CFL maximum mx holds (MEMB)
   const R h = R(0.5) * scale;
+  const R cw0 = (R)f.cflw0, cw1 = (R)f.cflw1, cw2 = (R)f.cflw2;
+  static_assert((E & (E - 1)) == 0, "power-of-two values per lane");
+  // lane of this pair holding bin N - k for k = j + G e (j > 0)
+  const int mirror = (lane & ~(G - 1)) | ((G - j) & (G - 1));
+  R mxr = R(0);  // running CFL maximum (as FP64 bits into maxbits when flushed)
   for (int it = 0; g < ngroups; g += TW, ++it) {
     long long mem = 0;
     if constexpr (MEMB) {
       mem = g / gpm;
       if (maxbits && mem != curm) {
-        if (curm >= 0) flush_max(maxbits, curm, mx);
+        if (curm >= 0) {
+          mx = (double)mxr;
+          mxr = R(0);
+          flush_max(maxbits, curm, mx);
+        }
         curm = mem;
       }
     }
@@ -514,30 +524,32 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
       c[0][e].x = u1.x * w2.x - u2.x * w1.x;  c[0][e].y = u1.y * w2.y - u2.y * w1.y;
       c[1][e].x = u2.x * w0.x - u0.x * w2.x;  c[1][e].y = u2.y * w0.y - u0.y * w2.y;
       c[2][e].x = u0.x * w1.x - u1.x * w0.x;  c[2][e].y = u0.y * w1.y - u1.y * w0.y;
-      if (maxbits) {
-        const double sa = fabs((double)u0.x) * f.cflw0 + fabs((double)u1.x) * f.cflw1 +
-                          fabs((double)u2.x) * f.cflw2;
-        const double sb = fabs((double)u0.y) * f.cflw0 + fabs((double)u1.y) * f.cflw1 +
-                          fabs((double)u2.y) * f.cflw2;
-        mx = fmax(mx, fmax(sa, sb));
+      if (maxbits) {  // CFL sums and their running maximum in the state's precision
+        const R sa = fabs(u0.x) * cw0 + fabs(u1.x) * cw1 + fabs(u2.x) * cw2;
+        const R sb = fabs(u0.y) * cw0 + fabs(u1.y) * cw1 + fabs(u2.y) * cw2;
+        mxr = fmax(mxr, fmax(sa, sb));
       }
     }
     const long long la = 2 * ((g - mem * gpm) * PW + pw);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
       fft<N, E, -1>(c[i], j, tw, smf, sync);
-#pragma unroll
-      for (int e = 0; e < E; ++e) smf(j + G * e) = c[i][e];
-      sync();
       C* oa = nl + i * f.nspec + la * f.nh;
       if constexpr (MEMB) oa += mem * 3 * f.nlcomp;
       C* ob = oa + f.nh;
+      // R2C split of the two lines: bin k = j + G e is this lane's register
+      // e; its mirror N - k is register E - 1 - e of lane G - j of the pair
+      // (register (E - e) mod E of this lane when j = 0), fetched by warp
+      // shuffles instead of a shared-memory round trip
 #pragma unroll
       for (int e = 0; e <= E / 2; ++e) {
+        C zn;
+        zn.x = __shfl_sync(0xffffffffu, c[i][E - 1 - e].x, mirror);
+        zn.y = __shfl_sync(0xffffffffu, c[i][E - 1 - e].y, mirror);
+        if (j == 0) zn = c[i][(E - e) & (E - 1)];
+        const C zk = c[i][e];
         const int k = j + G * e;
         if (k <= H) {
-          const C zk = smf(k);
-          const C zn = smf(k == 0 ? 0 : N - k);
           C Av, Bv;
           Av.x = (zk.x + zn.x) * h; Av.y = (zk.y - zn.y) * h;
           Bv.x = (zk.y + zn.y) * h; Bv.y = -(zk.x - zn.x) * h;
@@ -545,9 +557,9 @@ k_p3(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
           ob[k] = Bv;
         }
       }
-      sync();
     }
   }
+  mx = (double)mxr;
   if constexpr (MEMB) {
     if (maxbits && curm >= 0) flush_max(maxbits, curm, mx);
   } else if (maxbits) {
@@ -635,6 +647,7 @@ k_p3s(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
   double mx = 0.0;
   [[maybe_unused]] long long curm = -1;  // member whose CFL maximum mx holds (MEMB)
   const R h = R(0.5) * scale;
+  const R cw0 = (R)f.cflw0, cw1 = (R)f.cflw1, cw2 = (R)f.cflw2;
   for (int it = 0; g < ngroups; g += TW, ++it) {
     long long mem = 0;
     if constexpr (MEMB) {
@@ -663,11 +676,10 @@ k_p3s(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
 #pragma unroll
       for (int e = 0; e < E; ++e) {
         const C u0 = ur[j + G * e], u1 = ur[N + j + G * e], u2 = ur[2 * N + j + G * e];
-        const double sa = fabs((double)u0.x) * f.cflw0 + fabs((double)u1.x) * f.cflw1 +
-                          fabs((double)u2.x) * f.cflw2;
-        const double sb = fabs((double)u0.y) * f.cflw0 + fabs((double)u1.y) * f.cflw1 +
-                          fabs((double)u2.y) * f.cflw2;
-        mx = fmax(mx, fmax(sa, sb));
+        // CFL sums in the state's precision, the running maximum in FP64
+        const R sa = fabs(u0.x) * cw0 + fabs(u1.x) * cw1 + fabs(u2.x) * cw2;
+        const R sb = fabs(u0.y) * cw0 + fabs(u1.y) * cw1 + fabs(u2.y) * cw2;
+        mx = fmax(mx, (double)fmax(sa, sb));
       }
     }
     C c[3][E];

@@ -87,7 +87,7 @@ template <int N, int W>
 __global__ void __launch_bounds__(32 * W, 1)
 k_p3q(const float2* __restrict__ B, float2* __restrict__ nl, FGeo f,
       const float2* __restrict__ tw, unsigned long long* __restrict__ maxbits, float scale,
-      int* __restrict__ err, int ngroups) {
+      int* __restrict__ err, long long ngroups) {
   using T = TuneQ<N>;
   constexpr int E = T::E, G = T::G, PW = T::PW, R1 = T::R1, Q1 = T::Q1;
   constexpr int H = N / 2;
@@ -100,7 +100,7 @@ k_p3q(const float2* __restrict__ B, float2* __restrict__ nl, FGeo f,
   const int WC = T::warp_complex(f.c2);
   const uint32_t fbytes = (uint32_t)(fb * sizeof(float2));
   const long long fs_in = (long long)f.n0 * f.n1 * f.c2;
-  const int gpm = f.n0 * f.n1 / (2 * PW);  // groups per member
+  const long long gpm = (long long)f.n0 * f.n1 / (2 * PW);  // groups per member
   uint64_t* bar = reinterpret_cast<uint64_t*>(smraw) + warp;
   float2* wbase = reinterpret_cast<float2*>(smraw + 128) + (long long)warp * WC;
   float2* ex = wbase + SC + pw * T::BUF;
@@ -115,12 +115,12 @@ k_p3q(const float2* __restrict__ B, float2* __restrict__ nl, FGeo f,
   for (int q = 0; q < Q1; ++q)
 #pragma unroll
     for (int r = 1; r < R1; ++r) tq[q][r - 1] = __ldg(tw + r * (j + q * G));
-  auto issue = [&](int grp) {
+  auto issue = [&](long long grp) {
     if (lane == 0) {
       fence_proxy_async_smem();
       mbar_arrive_expect_tx(bar, 6 * fbytes);
-      const int mem = grp / gpm;  // member of the group
-      const float2* src = B + (long long)mem * 6 * fs_in + (long long)(grp - mem * gpm) * fb;
+      const long long mem = grp / gpm;  // member of the group
+      const float2* src = B + mem * 6 * fs_in + (grp - mem * gpm) * fb;
 #pragma unroll
       for (int fld = 0; fld < 6; ++fld) bulk_g2s(wbase + fld * fb, src + fld * fs_in, fbytes, bar);
     }
@@ -147,13 +147,13 @@ k_p3q(const float2* __restrict__ B, float2* __restrict__ nl, FGeo f,
   const float h = 0.5f * scale;
   // lane of this pair holding position N - k for k = j + G e (j > 0)
   const int mirror = (lane & ~(G - 1)) | ((G - j) & (G - 1));
-  const int TW = gridDim.x * W;  // groups of all members: below 2^31 (checked at plan creation)
-  int g = blockIdx.x * W + warp;
+  const long long TW = (long long)gridDim.x * W;
+  long long g = (long long)blockIdx.x * W + warp;
   if (g < ngroups) issue(g);
   float mx = 0.f;
-  int curm = -1;  // member whose CFL maximum mx holds
+  long long curm = -1;  // member whose CFL maximum mx holds
   // warp maximum into member m's slot as FP64 bits
-  auto flush = [&](int m) {
+  auto flush = [&](long long m) {
     double d = (double)mx;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) d = fmax(d, __shfl_xor_sync(0xffffffffu, d, o));
@@ -161,7 +161,7 @@ k_p3q(const float2* __restrict__ B, float2* __restrict__ nl, FGeo f,
     mx = 0.f;
   };
   for (int it = 0; g < ngroups; g += TW, ++it) {
-    const int mem = g / gpm;
+    const long long mem = g / gpm;
     if (maxbits && mem != curm) {
       if (curm >= 0) flush(curm);
       curm = mem;
@@ -214,11 +214,11 @@ k_p3q(const float2* __restrict__ B, float2* __restrict__ nl, FGeo f,
         c[ib][e].x -= ua.x * v[e].x;  c[ib][e].y -= ua.y * v[e].y;
       }
     }
-    const long long la = 2 * ((long long)(g - mem * gpm) * PW + pw);
+    const long long la = 2 * ((g - mem * gpm) * PW + pw);
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
       fft_q<N, -1>(c[i], j, tq, ex);
-      float2* oa = nl + ((long long)mem * 3 + i) * f.nlcomp + la * f.nh;
+      float2* oa = nl + (mem * 3 + i) * f.nlcomp + la * f.nh;
       float2* ob = oa + f.nh;
 #pragma unroll
       for (int e = 0; e <= E / 2; ++e) {
@@ -258,8 +258,7 @@ static cudaError_t p3q_run(const float2* B, float2* nl, const FGeo& f, const flo
   if (e != cudaSuccess) return e;
   long long blocks = (ngroups + W - 1) / W;
   if (blocks > nsm) blocks = nsm;
-  k_p3q<N, W><<<(unsigned)blocks, 32 * W, sm, st>>>(B, nl, f, tw, maxbits, scale, err,
-                                                      (int)ngroups);
+  k_p3q<N, W><<<(unsigned)blocks, 32 * W, sm, st>>>(B, nl, f, tw, maxbits, scale, err, ngroups);
   return launched();
 }
 
