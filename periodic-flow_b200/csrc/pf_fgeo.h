@@ -30,4 +30,10 @@ cudaError_t p3q_launch(int n2, int W, const float2* B, float2* nl, const FGeo& f
                        long long ngroups, int nsm, cudaStream_t st);
 bool p3q_supported(int n2, int W);
 
+// P2 of the 2/3 rule in FP32 at axis-1 length 256 with tiled bulk tensor
+// copies of its input tiles (pf_p2t.cu); one box: single-box plans only.
+cudaError_t p2t_launch(const float2* A, float2* B, const FGeo& f, const float2* tw, int* err,
+                       cudaStream_t st);
+bool p2t_supported(const FGeo& f);
+
 }  // namespace pf

@@ -205,6 +205,7 @@ static std::vector<int> candidates(const FusedPlan* p, int pass, bool& is384) {
   if (len == 256) {
     c = {0, 1, 2, 3, 4, 5, 6};
     if (pass == 2) c.insert(c.end(), {7, 8, 9});
+    if (pass == 2 && !p->pad && p2t_supported(f)) c.push_back(10);
     if (pass == 1) c.insert(c.end(), {7, 9});
   } else if (len == 384) {
     is384 = true;

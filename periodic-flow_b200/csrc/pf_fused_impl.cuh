@@ -1097,6 +1097,13 @@ template <typename R, int N, bool PAD> static cudaError_t p2_n(FusedPlan* p, cud
       case 7: return p2six_run<R, PAD, 256, 16, 8>(p, st);
       case 8: return p2six_run<R, PAD, 256, 16, 8, 4>(p, st);
       case 9: return p2six_run<R, PAD, 256, 16, 16>(p, st);
+      case 10:  // input tiles by tiled bulk tensor copies (pf_p2t.cu)
+        if constexpr (!PAD) {
+          if (p2t_supported(p->f))
+            return p2t_launch((const float2*)p->A, (float2*)p->B, p->f,
+                              tw_base<float>() + tw_offset(256), p->err, st);
+        }
+        break;
       default: break;
     }
   }

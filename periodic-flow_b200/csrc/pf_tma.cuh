@@ -14,7 +14,7 @@ namespace pf {
 // ~1 s at 1.9 GHz
 constexpr long long kWaitCycles = 2000000000LL;
 
-enum DeviceError { kErrNone = 0, kErrWaitP3 = 3 };
+enum DeviceError { kErrNone = 0, kErrWaitP2 = 2, kErrWaitP3 = 3 };
 
 PF_D uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 

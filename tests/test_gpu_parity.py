@@ -330,7 +330,7 @@ def test_autotune_keeps_state_and_parity():
     before = a.space_solver.u_hat
     picks = a.space_solver.autotune()
     assert np.array_equal(a.space_solver.u_hat, before)
-    built = {1: range(0, 10), 2: range(0, 10), 3: range(0, 6), 4: range(0, 7)}
+    built = {1: range(0, 10), 2: range(0, 11), 3: range(0, 6), 4: range(0, 7)}
     assert all(picks["axes_256"][p] in built[p] for p in built)
     assert a.space_solver.fused_variants() == picks
     a.space_solver.step(1)
@@ -368,6 +368,39 @@ def test_p3_one_exchange_form_vs_oracle(N, var, monkeypatch):
     b.initialize(uh0, "fourier")
     b.space_solver.step(2)
     assert rel_l2(a.space_solver.u_hat, b.space_solver.u_hat) < 2e-6
+
+
+@pytest.mark.parametrize("N", [(16, 256, 256), (48, 256, 64), (256, 256, 256)])
+def test_p2_tma_tiles_vs_oracle_and_plain_loads(N, monkeypatch):
+    """P2 with its input tiles brought in by tiled bulk tensor copies (rows
+    of c2 = 86 or 22 complex: multiples of 16 bytes): the same results as P2
+    with plain loads to rounding, and the FP64 oracle (forcing + CFL, 2
+    steps; 1 step at 256^3 against the per-operator path)."""
+    kw = dict(dt=1e-3, time_integrator="rk3", viscosity=2e-3, precision="fp32",
+              forcing=(0.1, 2.5), cfl=0.5)
+    uh0 = O.spectral_random_field(O.Grid(N), 8)
+    steps = 1 if N[0] == 256 else 2
+    out = {}
+    for var in (10, 0):
+        monkeypatch.setenv("PF_FUSED_VARIANT", f"p2:{var}")
+        a = solver(N, fused=True, **kw)
+        assert a.space_solver.fused_variants()["axes_256"][2] == var
+        a.initialize(uh0, "fourier")
+        a.space_solver.step(steps)
+        out[var] = a.space_solver.u_hat
+        del a
+    assert rel_l2(out[10], out[0]) < 1e-6
+    if N[0] == 256:
+        b = solver(N, fused=False, **kw)
+        b.initialize(uh0, "fourier")
+        b.space_solver.step(steps)
+        assert rel_l2(out[10], b.space_solver.u_hat) < 2e-6
+    else:
+        o = O.OracleSolver(N, 1e-3, time_integrator="rk3", viscosity=2e-3, forcing=(0.1, 2.5),
+                           cfl=0.5)
+        o.initialize(uh0, "fourier")
+        o.advance(steps)
+        assert rel_l2(out[10], o.u_hat) < 1e-5
 
 
 @pytest.mark.parametrize("var", [4, 5])
