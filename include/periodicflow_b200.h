@@ -254,6 +254,44 @@ int pf_set_active_members(pf_solver* h, int active);
 int pf_copy_member(pf_solver* h, int dst, int src);
 int pf_set_time_member(pf_solver* h, int member, double t, double dt);
 
+/* ---- slab decomposition of one box ---------------------------------------
+ * Replaces the reference's decomposition='slab' (basis.py:64, the shenfun
+ * TensorProductSpace with slab=True built over simulation.py:81-83's
+ * COMM_WORLD): the box is split into S slabs; slab r holds the spectral rows
+ * k1 in [r n1/S, (r+1) n1/S) of every (k0, k2) -- its u_hat is the local
+ * array [3][n0][n1/S][n2/2+1] complex128 -- and, between the transposes of
+ * the nonlinear term, the physical planes x0 in [r n0/S, (r+1) n0/S).  The
+ * transposes are stores of the passes before them into the destination
+ * slab's buffers.  Built for the 3D nonlinear problem with the 2/3 rule
+ * (FP32, FP64; the fused-schedule sides), every integrator, CFL dt, band
+ * forcing, Nyquist mask and thermal Philox noise (draws equal to a single
+ * box's); S <= 8 dividing n0 and n1, (n0/S) n1 a multiple of 64.
+ *
+ * pf_slab_create_group holds all S slabs in this process on the current
+ * device.  pf_slab_create holds slab `slab` only (one process per GPU):
+ * every process exports its exchange buffers (pf_slab_export, CUDA IPC
+ * handles), process 0 makes an NCCL id (pf_slab_nccl_id, 128 bytes), both
+ * are shared (e.g. by an MPI allgather / bcast), and pf_slab_connect maps the
+ * peers' buffers and joins the NCCL communicator that carries the exchange
+ * barriers and the CFL / forcing reductions.  pf_slab_step is collective. */
+typedef struct pf_slab pf_slab;
+int pf_slab_layout(int n0, int n1, int slabs, int slab, int* out6);  /* n0/S, n1/S, x0 first, k1 first, kept compact k1 first, count */
+int pf_slab_create_group(const pf_config* cfg, int slabs, pf_slab** out);
+int pf_slab_create(const pf_config* cfg, int slabs, int slab, pf_slab** out);
+int pf_slab_export(const pf_slab* h, void* out, size_t cap, size_t* used);
+int pf_slab_nccl_id(void* out, size_t cap);
+int pf_slab_connect(pf_slab* h, const void* exports, const void* nccl_id);  /* exports: S blocks in slab order */
+int pf_slab_destroy(pf_slab* h);
+const char* pf_slab_last_error(const pf_slab* h);
+int pf_slab_set_stream(pf_slab* h, void* stream);
+int pf_slab_sizes(const pf_slab* h, int* first, int* count, long long* nspec);  /* slabs held, modes per slab */
+int pf_slab_set_fourier(pf_slab* h, int slab, const double* u_hat, int where);
+int pf_slab_get_fourier(pf_slab* h, int slab, double* u_hat, int where);
+int pf_slab_step(pf_slab* h, int nsteps);
+int pf_slab_sync(pf_slab* h);
+int pf_slab_get_time(pf_slab* h, double* t, long long* step, double* dt);
+int pf_slab_energy(pf_slab* h, int slab, double* energy, double* enstrophy);  /* the slab's part */
+
 /* ---- backward transform without device allocation ----------------------
  * No counterpart in the reference: an addition for callers that cannot call
  * cudaMalloc (a fixed memory budget handed over by an embedding application,

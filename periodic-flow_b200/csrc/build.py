@@ -83,7 +83,7 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
         with ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
             list(ex.map(compile_one, todo))
     if force or todo or not os.path.exists(LIB) or os.path.getmtime(LIB) < _newest(objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-ldl"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")

@@ -630,6 +630,33 @@ static int validate(const pf_config* c) {
   return PF_OK;
 }
 
+}  // extern "C"
+
+int pf::config_validate(const pf_config* c) { return validate(c); }
+
+// Box geometry of a configuration (wavenumber scales 2 pi / L, 2/3-rule kmax).
+Geo pf::config_geo(const pf_config* cfg) {
+  Geo g;
+  memset(&g, 0, sizeof(g));
+  const int d = cfg->dim;
+  g.dim = d;
+  g.n[2] = 1;
+  for (int a = 0; a < d; ++a) {
+    g.n[a] = cfg->n[a];
+    g.kscale[a] = 2.0 * M_PI / (cfg->domain[a][1] - cfg->domain[a][0]);
+    g.kmax[a] = (cfg->n[a] - 1) / 3;
+    g.s[a] = cfg->n[a];
+  }
+  g.nh = cfg->n[d - 1] / 2 + 1;
+  g.s[d - 1] = g.nh;
+  g.nspec = 1;
+  g.nphys = 1;
+  for (int a = 0; a < d; ++a) { g.nspec *= g.s[a]; g.nphys *= g.n[a]; }
+  return g;
+}
+
+extern "C" {
+
 static int create_impl(const pf_config* cfg, int nmem, pf_solver** out) {
   if (!cfg || !out) return fail(nullptr, PF_ERR_INVALID, "pf_create: null argument");
   *out = nullptr;
@@ -653,21 +680,8 @@ static int create_impl(const pf_config* cfg, int nmem, pf_solver** out) {
   h->prec = cfg->precision;
   h->rsz = h->prec == PF_FP64 ? 8 : 4;
   h->ncomp = cfg->noise_type == PF_NOISE_THERMAL ? h->d * h->d : h->d;
+  h->g = pf::config_geo(cfg);
   Geo& g = h->g;
-  memset(&g, 0, sizeof(g));
-  g.dim = h->d;
-  g.n[2] = 1;
-  for (int a = 0; a < h->d; ++a) {
-    g.n[a] = cfg->n[a];
-    g.kscale[a] = 2.0 * M_PI / (cfg->domain[a][1] - cfg->domain[a][0]);
-    g.kmax[a] = (cfg->n[a] - 1) / 3;
-    g.s[a] = cfg->n[a];
-  }
-  g.nh = cfg->n[h->d - 1] / 2 + 1;
-  g.s[h->d - 1] = g.nh;
-  g.nspec = 1;
-  g.nphys = 1;
-  for (int a = 0; a < h->d; ++a) { g.nspec *= g.s[a]; g.nphys *= g.n[a]; }
   const size_t cb = 2 * h->rsz;  // complex bytes
   auto alloc = [&](void** p, size_t bytes) -> bool {
     if (cudaMalloc(p, bytes) != cudaSuccess) return false;

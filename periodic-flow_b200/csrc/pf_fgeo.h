@@ -19,7 +19,18 @@ struct FGeo {
   // buffer (state 3 nspec, nl 3 nlcomp, A 5 t0 c1 c2, B 6 t0 t1 c2 complex
   // values per member); each pass covers all of them in one launch.
   int nmem;
+  // Slab decomposition of one box over sl_S slabs (pf_slab.cu; unused by the
+  // whole-box passes): slab r holds the spectral rows k1 in [r sl_n1,
+  // (r + 1) sl_n1) of every (k0, k2) and, between the two exchanges, the
+  // physical planes x0 in [r sl_n0, (r + 1) sl_n0).  P1 of a slab transforms
+  // its kept compact rows [sl_c0, sl_c0 + sl_nc) and stores plane x0 straight
+  // into slab x0 / sl_n0's pass-1 buffer sl_dst[x0 / sl_n0]; P4 stores row k1
+  // into slab k1 / sl_n1's nonlinear buffer.  sl_dst may be another GPU's
+  // memory (peer mapping): plain stores only.
+  int sl_S, sl_n0, sl_n1, sl_x0, sl_i1, sl_c0, sl_nc, sl_N0;
+  void* sl_dst[8];
 };
+constexpr int kMaxSlabs = 8;
 
 // P3 of the 2/3 rule in FP32 with one shared-memory exchange per line FFT
 // (pf_p3q.cu): contiguous sides n2 = 128 or 256, W warps per CTA (6 or 7),

@@ -41,11 +41,9 @@ static FusedPlan* fused_create_2d(const Geo& g, int precision, int nmem) {
   return p;
 }
 
-FusedPlan* fused_create(const Geo& g, int precision, int dealias, int nmem) {
-  if ((precision != 0 && precision != 1) || (dealias != 0 && dealias != 1) || nmem < 1)
-    return nullptr;
-  // 2D: 2/3 rule, sides 2^b 16..1024, FP32 and FP64
-  if (g.dim == 2) return dealias == 0 ? fused_create_2d(g, precision, nmem) : nullptr;
+// slabs > 1: the pencil plan of one slab of the box (passes 2-4 on its
+// n0 / slabs planes; pf_slab.cu)
+static FusedPlan* create3d(const Geo& g, int precision, int dealias, int nmem, int slabs) {
   if (g.dim != 3) return nullptr;
   const bool pad = dealias == 1;
   // FP32 2/3 rule: sides 2^b 16..512 (the last up to 256) and 3 * 2^b
@@ -81,6 +79,16 @@ FusedPlan* fused_create(const Geo& g, int precision, int dealias, int nmem) {
   f.cflw1 = g.n[1] * g.kscale[1] / (2.0 * M_PI);
   f.cflw2 = g.n[2] * g.kscale[2] / (2.0 * M_PI);
   f.nspec = g.nspec;
+  if (slabs > 1) {
+    if (pad || nmem != 1 || f.n0 % slabs != 0) {
+      delete p;
+      return nullptr;
+    }
+    p->slabs = slabs;
+    f.n0 = f.t0 = f.n0 / slabs;
+    f.nlcomp = (long long)f.t0 * f.t1 * f.nh;
+    f.nspec = f.nlcomp;
+  }
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tuned.find(tune_key(p));
@@ -125,6 +133,19 @@ FusedPlan* fused_create(const Geo& g, int precision, int dealias, int nmem) {
     return nullptr;
   }
   return p;
+}
+
+FusedPlan* fused_create(const Geo& g, int precision, int dealias, int nmem) {
+  if ((precision != 0 && precision != 1) || (dealias != 0 && dealias != 1) || nmem < 1)
+    return nullptr;
+  // 2D: 2/3 rule, sides 2^b 16..1024, FP32 and FP64
+  if (g.dim == 2) return dealias == 0 ? fused_create_2d(g, precision, nmem) : nullptr;
+  return create3d(g, precision, dealias, nmem, 1);
+}
+
+FusedPlan* fused_create_pencil(const Geo& g, int precision, int slabs) {
+  if ((precision != 0 && precision != 1) || slabs < 2) return nullptr;
+  return create3d(g, precision, 0, 1, slabs);
 }
 
 void fused_set_members(FusedPlan* p, int active) {

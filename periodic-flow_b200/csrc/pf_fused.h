@@ -15,6 +15,11 @@ struct FusedPlan;
 // nmem > 1: buffers and launches for nmem boxes of this geometry laid out one
 // after another (state, nl and the device scalars of the caller likewise).
 FusedPlan* fused_create(const Geo& g, int precision, int dealias, int nmem = 1);
+// The pencil plan of one of `slabs` slabs of a 3D box (2/3 rule): passes 2-4
+// on n0 / slabs planes x0 (pass-1 buffer A [5][n0/slabs][c1][c2], nl in the
+// layout [3][n0/slabs][n1][nh]); pass 3 scales by 1 / (n0 n1 n2).  nullptr
+// where fused_create(g, precision, 0) has no plan or slabs does not divide n0.
+FusedPlan* fused_create_pencil(const Geo& g, int precision, int slabs);
 void fused_destroy(FusedPlan* p);
 // Launches of the plan cover members [0, active) (active <= the plan's members).
 void fused_set_members(FusedPlan* p, int active);

@@ -123,6 +123,7 @@ struct FusedPlan {
   F2 f2;
   int* err = nullptr; // device error word (bounded waits that gave up)
   int cap = 1;        // members the buffers hold (f.nmem / f2.nmem: members launched)
+  int slabs = 1;      // pencil plan of one slab (pf_slab.cu): f.n0 = f.t0 = planes per slab
   int nsm = 148;
   // launch variant per pass (used where that pass's axis has 256 points):
   // measured best on B200 at 256^3 are P1 one output field per CTA row
@@ -151,8 +152,21 @@ PF_D void flush_max(unsigned long long* maxbits, long long m, double& mx) {
   mx = 0.0;
 }
 
+// Destination slab s of a slab pass's store: selects among the (kernel
+// parameter) pointers with constant indices.
+template <typename C> PF_D C* slab_dst(const FGeo& f, int s) {
+  void* p = f.sl_dst[0];
+#pragma unroll
+  for (int i = 1; i < kMaxSlabs; ++i)
+    if (s == i) p = f.sl_dst[i];
+  return reinterpret_cast<C*>(p);
+}
+
 // ---------------------------------------------------------------------- P1
-template <typename R, int N, int E, int T, int MB, bool PAD, bool FIVE = false, bool MEMB = false>
+// SLAB (with FIVE, 2/3 rule): one slab's kept compact rows; plane x0 of the
+// output goes to slab x0 / sl_n0's pass-1 buffer [5][sl_n0][c1][c2].
+template <typename R, int N, int E, int T, int MB, bool PAD, bool FIVE = false, bool MEMB = false,
+          bool SLAB = false>
 __global__ void __launch_bounds__(T * (N / E), MB)
 k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
      const cx<R>* __restrict__ tw) {
@@ -166,18 +180,20 @@ k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
     uh += (long long)blockIdx.z * 3 * f.nspec;
     A += (long long)blockIdx.z * 5 * f.t0 * f.c1 * f.c2;
   }
+  static_assert(!SLAB || (FIVE && !PAD && !MEMB), "slab P1: one field per CTA row, 2/3 rule");
   const int t = threadIdx.x, j = threadIdx.y;
-  const int ncols = f.c1 * f.c2;
+  const int ncols = (SLAB ? f.sl_nc : f.c1) * f.c2;
   const int q = blockIdx.x * T + t;
   const bool active = q < ncols;
   int in_off = 0;
   if (active) {
-    const int k1c = q / f.c2;
+    int k1c = q / f.c2;
     const int k2c = q - k1c * f.c2;
+    if constexpr (SLAB) k1c += f.sl_c0;
     const int i1 = k1c <= f.kmax1 ? k1c : k1c + (f.n1 - f.c1);
-    in_off = i1 * f.nh + k2c;
+    in_off = (SLAB ? i1 - f.sl_i1 : i1) * f.nh + k2c;
   }
-  const int row_in = f.n1 * f.nh;
+  const int row_in = (SLAB ? f.sl_n1 : f.n1) * f.nh;
   const int fs_out = N * ncols;
   const int fs_in = (int)f.nspec;
   auto smf = [&](int pos) -> C& { return sm[col_pos<T>(pos, t)]; };
@@ -212,7 +228,20 @@ k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
       if (fld >= 3) w[e] = cmuli(cscale(w[e], (R)(f.ks0 * kf)));
     }
     fft<N, E, +1>(w, j, tw, smf, sync);
-    if (active) {
+    if constexpr (SLAB) {
+      const int plane = f.c1 * f.c2;
+      const long long fsd = (long long)f.sl_n0 * plane;
+      const int col = f.sl_c0 * f.c2 + q;
+      if (active) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const int x0 = j + G * e, s = x0 / f.sl_n0;
+          slab_dst<C>(f, s)[fld * fsd + (long long)(x0 - s * f.sl_n0) * plane + col] = w[e];
+        }
+      }
+      // the stores may go to peer memory: visible before the exchange barrier
+      __threadfence_system();
+    } else if (active) {
 #pragma unroll
       for (int e = 0; e < E; ++e) A[fld * fs_out + (j + G * e) * ncols + q] = w[e];
     }
@@ -749,7 +778,9 @@ k_p3s(const cx<R>* __restrict__ B, cx<R>* __restrict__ nl, FGeo f,
 // k2) with plane = comp * t0 + x0.  3/2 rule: the t1 transform rows are then
 // truncated to the n1 N-grid rows (+n1/2 and -n1/2 folded into the Nyquist
 // row), written to the first n1 rows of the column.
-template <typename R, int N, int E, int T, int MB, bool PAD, bool MEMB = false>
+// SLAB (2/3 rule): out of place, row k1 of the column to slab k1 / sl_n1's
+// nonlinear buffer [3][sl_N0][sl_n1][nh] at plane sl_x0 + x0.
+template <typename R, int N, int E, int T, int MB, bool PAD, bool MEMB = false, bool SLAB = false>
 __global__ void __launch_bounds__(T * (N / E), MB)
 k_p4(cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
   constexpr int G = N / E;
@@ -772,7 +803,22 @@ k_p4(cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
     v[e] = active ? nl[base + (long long)(j + G * e) * f.nh] : czero<C>();
   fft<N, E, -1>(v, j, tw, [&](int pos) -> C& { return sm[col_pos<T>(pos, t)]; },
                 [] { __syncthreads(); });
-  if constexpr (!PAD) {
+  if constexpr (SLAB) {
+    static_assert(!PAD && !MEMB, "slab P4: 2/3 rule");
+    if (active) {
+      const long long pl = q / f.nh;
+      const int c = (int)(pl / f.t0), xl = (int)(pl - (long long)c * f.t0);
+      const long long rows = (long long)f.sl_n1 * f.nh;
+      const long long bd = c * (long long)f.sl_N0 * rows + (long long)(f.sl_x0 + xl) * rows +
+                           (q - pl * f.nh);
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int i = j + G * e, r = i / f.sl_n1;
+        slab_dst<C>(f, r)[bd + (long long)(i - r * f.sl_n1) * f.nh] = v[e];
+      }
+    }
+    __threadfence_system();
+  } else if constexpr (!PAD) {
     if (active) {
 #pragma unroll
       for (int e = 0; e < E; ++e) nl[base + (long long)(j + G * e) * f.nh] = v[e];
@@ -801,7 +847,10 @@ k_p4(cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
 // N x T buffer per component, also the FFT's exchange buffer) so the update
 // phase holds only a chunk of modes in registers; u_hat / u0 of a chunk are
 // loaded before any of its stores.
-template <typename R, int N, int NC, bool NOISE, int CHU, bool PAD, bool MEMB = false>
+// SLAB: the columns of one slab's k1 rows [sl_i1, sl_i1 + sl_n1) (state and
+// nl in the slab's layout; wavenumbers and noise sites of the whole box).
+template <typename R, int N, int NC, bool NOISE, int CHU, bool PAD, bool MEMB = false,
+          bool SLAB = false>
 __global__ void __launch_bounds__(TuneU<N, R>::T * TuneU<N, R>::G, sizeof(R) == 8 ? 1 : 2)
 k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
   constexpr int E = TuneU<N, R>::E, G = TuneU<N, R>::G, T = TuneU<N, R>::T;
@@ -812,7 +861,7 @@ k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restr
   extern __shared__ __align__(16) unsigned char smraw[];
   C* S = reinterpret_cast<C*>(smraw);
   const int t = threadIdx.x, j = threadIdx.y;
-  const int ncols = f.n1 * f.nh;
+  const int ncols = (SLAB ? f.sl_n1 : f.n1) * f.nh;
   const int q = blockIdx.x * T + t;
   const bool active = q < ncols;
   const long long fs = f.nlcomp;  // nl: [3][t0][rows of nlrow]; 2/3 rule: the state layout
@@ -855,7 +904,8 @@ k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restr
   const StageScalars<R> sc = stage_scalars<R>(U, mem.mb);
   double accE = 0.0, accZ = 0.0;
   if (active) {
-    const int i1 = q / f.nh, i2 = q - i1 * f.nh;
+    const int i1l = q / f.nh, i2 = q - i1l * f.nh;
+    const int i1 = SLAB ? i1l + f.sl_i1 : i1l;
     const R k1 = (R)(f.ks1 * kfreq(i1, f.n1)), k2 = (R)(f.ks2 * i2);
     cx<R>* __restrict__ uh = U.uhat + mem.mo;
     cx<R>* __restrict__ u0p = U.u0 + mem.mo;
@@ -1133,7 +1183,7 @@ static cudaError_t p3s_run(FusedPlan* p, cx<R>* nl, unsigned long long* maxbits,
   const size_t sm = 128 + sizeof(cx<R>) * (size_t)W * WC;
   cudaError_t e = set_smem(k_p3s<R, N, W, PAD>, sm);
   if (e != cudaSuccess) return e;
-  const R scale = (R)(1.0 / ((double)p->f.t0 * p->f.t1 * p->f.t2));
+  const R scale = (R)(1.0 / ((double)p->f.t0 * p->slabs * p->f.t1 * p->f.t2));
   long long blocks = (ngroups + W - 1) / W;
   if (blocks > (long long)p->nsm) blocks = p->nsm;
   if (p->f.nmem > 1) {
@@ -1159,7 +1209,7 @@ static cudaError_t p3_run(FusedPlan* p, float2* nl, unsigned long long* maxbits,
   const size_t sm = 128 + sizeof(float2) * (size_t)W * WC;
   cudaError_t e = set_smem(k_p3<float, N, NB, W, MB>, sm);
   if (e != cudaSuccess) return e;
-  const float scale = (float)(1.0 / ((double)p->f.n0 * p->f.n1 * p->f.n2));
+  const float scale = (float)(1.0 / ((double)p->f.n0 * p->slabs * p->f.n1 * p->f.n2));
   long long blocks = (ngroups + W - 1) / W;
   if (blocks > (long long)p->nsm * MB) blocks = (long long)p->nsm * MB;
   if (p->f.nmem > 1) {
@@ -1181,7 +1231,7 @@ static inline cudaError_t p3q_go(FusedPlan* p, int n, int W, float2* nl, unsigne
   const float2* tw = tw_base<float>() + tw_offset(n);
   const int pw = 32 / (n / 16);
   const long long ngroups = (long long)p->f.nmem * p->f.n0 * p->f.n1 / (2 * pw);
-  const float scale = (float)(1.0 / ((double)p->f.n0 * p->f.n1 * p->f.n2));
+  const float scale = (float)(1.0 / ((double)p->f.n0 * p->slabs * p->f.n1 * p->f.n2));
   return p3q_launch(n, W, (const float2*)p->B, nl, p->f, tw, maxbits, scale, p->err, ngroups,
                     p->nsm, st);
 }

@@ -6,10 +6,16 @@
 
 #include "pf_common.cuh"
 
+struct pf_config;
+
 namespace pf {
 
 // Record the message returned by pf_last_error(NULL); returns code.
 int set_static_error(int code, const std::string& msg);
+// The checks pf_create applies to a configuration (PF_OK or an error code,
+// message via pf_last_error(NULL)), and the box geometry it describes.
+int config_validate(const ::pf_config* c);
+Geo config_geo(const ::pf_config* c);
 
 struct SolverView;
 

@@ -45,6 +45,14 @@ class Comm:
         d.all_gather_object(out, value)
         return sum(out)
 
+    def allgather(self, obj):
+        d = self._dist()
+        if not d:
+            return [obj]
+        out = [None] * d.get_world_size()
+        d.all_gather_object(out, obj)
+        return out
+
     def bcast(self, obj, root: int = 0):
         d = self._dist()
         if not d:

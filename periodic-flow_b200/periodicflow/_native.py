@@ -109,6 +109,25 @@ _SIGS = [
     ("pf_batch_capture", C.c_int, [C.c_void_p, C.c_int]),
     ("pf_batch_replay", C.c_int, [C.c_void_p]),
     ("pf_batch_sync", C.c_int, [C.c_void_p]),
+    ("pf_slab_layout", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    ("pf_slab_create_group", C.c_int, [C.POINTER(PfConfig), C.c_int, C.POINTER(C.c_void_p)]),
+    ("pf_slab_create", C.c_int, [C.POINTER(PfConfig), C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    ("pf_slab_export", C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    ("pf_slab_nccl_id", C.c_int, [C.c_void_p, C.c_size_t]),
+    ("pf_slab_connect", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("pf_slab_destroy", C.c_int, [C.c_void_p]),
+    ("pf_slab_last_error", C.c_char_p, [C.c_void_p]),
+    ("pf_slab_set_stream", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("pf_slab_sizes", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                C.POINTER(C.c_longlong)]),
+    ("pf_slab_set_fourier", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    ("pf_slab_get_fourier", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    ("pf_slab_step", C.c_int, [C.c_void_p, C.c_int]),
+    ("pf_slab_sync", C.c_int, [C.c_void_p]),
+    ("pf_slab_get_time", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
+                                   C.POINTER(C.c_double)]),
+    ("pf_slab_energy", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double),
+                                 C.POINTER(C.c_double)]),
     ("pf_op_cross", C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_longlong)] + [C.c_void_p] * 4),
     ("pf_op_curl", C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_longlong)] + [C.c_void_p] * 4),
     ("pf_op_apply_linear_operator", C.c_int,
@@ -147,9 +166,9 @@ def lib():
     return _lib
 
 
-def check(rc: int, handle=None, what: str = ""):
+def check(rc: int, handle=None, what: str = "", errfn=None):
     if rc != PF_OK:
-        msg = lib().pf_last_error(handle)
+        msg = (errfn or lib().pf_last_error)(handle)
         msg = msg.decode() if msg else ""
         if rc == 1:
             raise ValueError(f"{what}: {msg}")
