@@ -302,6 +302,9 @@ def run_ours(args, dist, rank, world):
     nlbatch = None
     if rank == 0 and not args.no_nlbatch and not pad:
         nlbatch = run_batched_nonlinear(args)
+    slabs = None
+    if rank == 0 and not args.no_slab and not pad:
+        slabs = run_slab_group(args, uh0)
     served = None
     if rank == 0 and not args.no_serving and not pad:
         served = run_serving(args)
@@ -335,6 +338,7 @@ def run_ours(args, dist, rank, world):
             "clocks": ck, "roofline": roofline, "step_roofline": step_roof,
             "e2e": e2e, "cpu_baseline": cpu, "oracle_check": check,
             "batched": ensemble, "batched_nonlinear": nlbatch, "served": served,
+            "slab_group": slabs,
             "padded_3_2": padded,
             "cufft_comparison": cufft, "fp64": fp64,
         }
@@ -759,6 +763,69 @@ def run_batched_nonlinear(args):
     return out
 
 
+def slab_exchange_bytes(n, S, cb=8):
+    """NVLink bytes one GPU sends per RK3 step when the n^3 box is split over S
+    GPUs: P1's planes for the other slabs (5 fields of the slab's kept
+    columns) and P4's rows for the other slabs (3 fields of its planes), per
+    stage."""
+    nh = n // 2 + 1
+    kmax = (n - 1) // 3
+    c1, c2 = 2 * kmax + 1, kmax + 1
+    frac = (S - 1) / S
+    e1 = 5 * n * (c1 / S) * c2 * cb * frac
+    e2 = 3 * (n / S) * n * nh * cb * frac
+    return 3 * (e1 + e2)
+
+
+def run_slab_group(args, uh0):
+    """The headline box split into S slabs held on this one GPU (pf_slab
+    group): ms per RK3 step of all slabs' kernels against the whole-box step
+    with the same plain launches, and the state difference.  The cross-slab
+    stores stay in this GPU's memory here; on S GPUs they cross NVLink
+    (bytes per GPU and step, and their time at the measured 770 GB/s peer
+    bandwidth, reported beside)."""
+    import torch
+    from periodicflow.slab import SlabGroup
+    n = args.n
+    steps = args.slab_steps
+    kw = dict(time_integrator=CFG["integrator"], viscosity=CFG["nu"], precision="fp32",
+              forcing=CFG["forcing"], cfl=CFG["cfl"])
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sol = make_solver(n)
+    ss = sol.space_solver
+    ss.initialize_velocity(uh0, "fourier")
+    ss.step(3)
+    torch.cuda.synchronize()
+    e0.record()
+    ss.step(steps)
+    e1.record()
+    torch.cuda.synchronize()
+    whole_ms = e0.elapsed_time(e1) / steps
+    ref = ss.u_hat
+    out = {"workload": f"{n}^3 forced RK3 CFL 0.5 FP32, {steps} steps after 3 warm-up, "
+                       "one recorded step replayed per step (both), every slab on this GPU",
+           "whole_box_ms_per_step": whole_ms, "slabs": {}}
+    for S in (2, 4, 8):
+        G = SlabGroup((n, n, n), CFG["dt0"], S, **kw)
+        G.set_state(uh0)
+        G.step(3)
+        torch.cuda.synchronize()
+        e0.record()
+        G.step(steps)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        diff = float(np.linalg.norm(G.state() - ref) / np.linalg.norm(ref))
+        b = slab_exchange_bytes(n, S)
+        out["slabs"][str(S)] = {"ms_per_step": ms, "vs_whole_box": whole_ms / ms,
+                                "rel_l2_vs_whole_box": diff,
+                                "nvlink_bytes_per_gpu_step": b,
+                                "nvlink_ms_at_770GBs": b / 770e9 * 1e3}
+        G.close()
+        del G
+    return out
+
+
 def cpu_baseline(n, steps, uh0):
     """The oracle (FP64 NumPy + scipy.fft on all host cores) on the same box,
     from the benchmark's initial field.  Returns the baseline record and the
@@ -910,6 +977,8 @@ def main():
     ap.add_argument("--no-nlbatch", action="store_true")
     ap.add_argument("--nlb-steps", type=int, default=200)
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-slab", action="store_true")
+    ap.add_argument("--slab-steps", type=int, default=10)
     ap.add_argument("--no-padded", action="store_true")
     ap.add_argument("--no-cufft", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")

@@ -131,6 +131,24 @@ def test_slab_solver_one_rank_through_nccl():
     s.close()
 
 
+def test_slab_group_graph_replay_equals_plain_steps():
+    """step(n >= 2) of a noise-free group replays one recorded step."""
+    from periodicflow.slab import SlabGroup
+    N = (64, 32, 32)
+    kw = dict(time_integrator="rk3", viscosity=2e-3, precision="fp32", forcing=(0.1, 2.5),
+              cfl=0.5)
+    uh = O.spectral_random_field(O.Grid(N), 8)
+    a, b = SlabGroup(N, 1e-3, 2, **kw), SlabGroup(N, 1e-3, 2, **kw)
+    a.set_state(uh)
+    b.set_state(uh)
+    for _ in range(4):
+        a.step(1)
+    b.step(2)
+    b.step(2)
+    assert np.array_equal(a.state(), b.state())
+    assert a.time() == b.time()
+
+
 def test_slab_group_local_layout():
     """Slab r holds rows k1 in [r n1/S, (r+1) n1/S) of the whole-box array."""
     from periodicflow.slab import SlabGroup, slab_layout
