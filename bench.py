@@ -57,10 +57,9 @@ def pass_bytes(n):
 
 
 # DRAM bytes (read + write) per launch at n = 256 from one ncu --set full
-# capture of k_p3 / k_p5 under "bench.py --steps 10 --warmup 3 --no-e2e
-# --no-cpu --no-ensemble --no-padded --no-cufft --no-autotune" with the
-# autotuner's picks (PF_FUSED_VARIANT=p1:3).
-NCU_TRAFFIC_256 = {3: 270.698496e6 + 157.537536e6, 5: 608.811008e6 + 172.103680e6}
+# capture per kernel of k_p3 / k_p5 (default launch forms) under
+# "bench.py --mode case --n 256 --steps 2".
+NCU_TRAFFIC_256 = {3: 270.720256e6 + 161.286400e6, 5: 608.809472e6 + 171.203072e6}
 
 
 def _dist():
