@@ -5,6 +5,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/periodicflow_b200.h"
@@ -63,20 +64,34 @@ struct pf_solver {
   long long graph_launches = 0;
   bool capturing = false;
   // private one-step graph of pf_step (noise-free, no history, no timer):
-  // recorded on its own stream, replayed once per step on st
-  cudaGraph_t agraph = nullptr;
-  cudaGraphExec_t agexec = nullptr;
+  // recorded on its own stream, replayed once per step on st; one per state
+  // buffer holding the current state (the roles swap every step)
+  cudaGraph_t agraph[2] = {nullptr, nullptr};
+  cudaGraphExec_t agexec[2] = {nullptr, nullptr};
   cudaStream_t astream = nullptr;
   long long a_launches = 0;
   bool auto_graph = true;
+  // One box on the fused schedule: the first stage of a step writes the new
+  // state into the u0 buffer and keeps the old one where it is as the step's
+  // u0 (no copy of the state); uhat and u0 then swap roles.  sbuf0 is the
+  // buffer that held the state at creation (parity 0).
+  bool swap_state = false;
+  void* sbuf0 = nullptr;
+  bool no_swap_next = false;  // the next recorded or run step keeps its buffers
+  int graph_parity = 0;       // state buffer the captured graph starts from
   std::string err;
 };
 
 // Kernel arguments recorded in the private step graph change: record again.
 static void drop_auto_graph(pf_solver* h) {
-  if (h->agexec) { cudaGraphExecDestroy(h->agexec); h->agexec = nullptr; }
-  if (h->agraph) { cudaGraphDestroy(h->agraph); h->agraph = nullptr; }
+  for (int p = 0; p < 2; ++p) {
+    if (h->agexec[p]) { cudaGraphExecDestroy(h->agexec[p]); h->agexec[p] = nullptr; }
+    if (h->agraph[p]) { cudaGraphDestroy(h->agraph[p]); h->agraph[p] = nullptr; }
+  }
 }
+
+// which state buffer holds the current state (0: the one it started in)
+static int state_parity(const pf_solver* h) { return h->uhat == h->sbuf0 ? 0 : 1; }
 
 // record an event on the solver stream when `pass` is the timed pass; events
 // come in (begin, end) pairs around each launch of that pass.  Inside a
@@ -368,14 +383,20 @@ static int step_generic(pf_solver* h) {
   const bool cfl = h->cfg.cfl > 0.0;
   const bool forcing = h->cfg.forcing_eps > 0.0;
   const bool use_fused = h->fused != nullptr && h->cfg.fused && h->cfg.is_nonlinear;
+  // the first stage writes the new state into the u0 buffer (roles swap)
+  const bool swap = use_fused && h->swap_state && !h->no_swap_next;
+  h->no_swap_next = false;
+  void* const old_state = h->uhat;
+  void* const new_state = swap ? h->u0 : h->uhat;
   for (int s = 0; s < sc.nstages; ++s) {
+    void* const cur = s == 0 ? old_state : new_state;  // the stage's input state
     if (h->cfg.is_nonlinear) {
       if (use_fused) {
         if (s == 0 && cfl)
           PF_CUDA(h, cudaMemsetAsync(h->maxbits, 0, sizeof(unsigned long long) * h->nact, h->st));
         for (int p = 1; p <= 4; ++p) {
           tmark(h, PF_PASS_FUSED_P1 + p - 1);
-          cudaError_t fe = fused_pass(h->fused, p, h->uhat, h->nl,
+          cudaError_t fe = fused_pass(h->fused, p, cur, h->nl,
                                       (s == 0 && cfl && p == 3) ? h->maxbits : nullptr, h->st);
           tmark(h, PF_PASS_FUSED_P1 + p - 1);
           PF_CUDA(h, fe);
@@ -390,13 +411,14 @@ static int step_generic(pf_solver* h) {
       return fail(h, PF_ERR_UNSUPPORTED, "CFL-adaptive dt needs the nonlinear term");
     }
     if (forcing)
-      PF_CUDA(h, launch_band_energy<R>((const cx<R>*)h->uhat, g,
+      PF_CUDA(h, launch_band_energy<R>((const cx<R>*)cur, g,
                                        h->cfg.forcing_kf * h->cfg.forcing_kf, h->dscal, h->st,
                                        h->nact));
     UpdateArgs<R> A;
     memset(&A, 0, sizeof(A));
-    A.uhat = (cx<R>*)h->uhat;
-    A.u0 = (cx<R>*)h->u0;
+    A.uhat = (cx<R>*)cur;
+    A.u0 = (cx<R>*)(swap ? old_state : h->u0);
+    A.uout = (swap && s == 0) ? (cx<R>*)new_state : nullptr;
     A.nl = h->cfg.is_nonlinear ? (const cx<R>*)h->nl : nullptr;
     A.lop = (const R*)h->lop;
     A.corr = (const R*)h->corr;
@@ -431,6 +453,7 @@ static int step_generic(pf_solver* h) {
     PF_CUDA(h, ue);
   }
   if (!cfl) PF_CUDA(h, launch_advance_time(h->dscal, 1, h->st, h->nact));
+  if (swap) std::swap(h->uhat, h->u0);
   return PF_OK;
 }
 
@@ -490,8 +513,12 @@ static int flush_hist(pf_solver* h) {
 template <typename R>
 static int record_auto_graph(pf_solver* h) {
   if (!h->astream) PF_CUDA(h, cudaStreamCreateWithFlags(&h->astream, cudaStreamNonBlocking));
+  const int par = state_parity(h);
+  void* const uhat = h->uhat;
+  void* const u0 = h->u0;
   cudaStream_t user = h->st;
   h->st = h->astream;
+  h->no_swap_next = false;
   const long long l0 = launch_total();
   h->capturing = true;
   cudaError_t e = cudaStreamBeginCapture(h->astream, cudaStreamCaptureModeThreadLocal);
@@ -501,13 +528,15 @@ static int record_auto_graph(pf_solver* h) {
     cudaGraph_t g = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(h->astream, &g);
     if (e == cudaSuccess) e = e2;
-    h->agraph = g;
+    h->agraph[par] = g;
   }
   h->capturing = false;
   h->st = user;
+  h->uhat = uhat;  // recorded, not run: the buffers keep their roles
+  h->u0 = u0;
   h->a_launches = launch_total() - l0;
   add_launches(-h->a_launches);  // recorded, not launched
-  if (rc == PF_OK && e == cudaSuccess) e = cudaGraphInstantiate(&h->agexec, h->agraph, 0);
+  if (rc == PF_OK && e == cudaSuccess) e = cudaGraphInstantiate(&h->agexec[par], h->agraph[par], 0);
   if (rc != PF_OK || e != cudaSuccess) {
     drop_auto_graph(h);
     cudaGetLastError();
@@ -532,16 +561,19 @@ static int step_impl(pf_solver* h, int nsteps) {
   const bool graphable = !stokes_fast && h->auto_graph && !injected && noise_src(h) == kNoiseNone &&
                          !h->record_hist && h->tpass < 0 && nsteps >= 2;
   if (graphable) {
-    if (!h->agexec) {
-      int rc = record_auto_graph<R>(h);
-      if (rc) return rc;
-    }
     for (; done < nsteps; ++done) {
-      PF_CUDA(h, cudaGraphLaunch(h->agexec, h->st));
+      const int par = state_parity(h);
+      if (!h->agexec[par]) {
+        int rc = record_auto_graph<R>(h);
+        if (rc) return rc;
+        if (!h->agexec[par]) break;  // recording failed: plain steps from here
+      }
+      PF_CUDA(h, cudaGraphLaunch(h->agexec[par], h->st));
       add_launches(h->a_launches);
       h->step += 1;
+      if (h->swap_state) std::swap(h->uhat, h->u0);
     }
-    return PF_OK;
+    if (done == nsteps) return PF_OK;
   }
   while (done < nsteps) {
     int chunk = nsteps - done;
@@ -731,6 +763,9 @@ static int create_impl(const pf_config* cfg, int nmem, pf_solver** out) {
   if (cfg->is_nonlinear && cfg->fused) {
     h->fused = fused_create(g, h->prec, cfg->dealias, nmem);  // nullptr when no fused path fits
   }
+  h->sbuf0 = h->uhat;
+  h->swap_state = h->fused != nullptr && nmem == 1;
+  if (const char* v = getenv("PF_STATE_SWAP")) h->swap_state = h->swap_state && atoi(v) != 0;
   if (nmem > 1 && !h->fused) {
     pf_destroy(h);
     return fail(nullptr, PF_ERR_UNSUPPORTED,
@@ -1228,6 +1263,9 @@ static int capture_steps(pf_solver* h, int nsteps) {
   const bool linear = !h->cfg.is_nonlinear && h->cfg.forcing_eps <= 0.0 && h->cfg.cfl <= 0.0;
   if (linear) return step_stokes<R>(h, nsteps);
   for (int i = 0; i < nsteps; ++i) {
+    // an odd count ends with a step that keeps its buffers, so the graph ends
+    // on the buffer it starts from and can be replayed again
+    h->no_swap_next = (nsteps & 1) && i == nsteps - 1;
     int rc = step_generic<R>(h);
     if (rc) return rc;
   }
@@ -1248,6 +1286,9 @@ extern "C" int pf_graph_capture(pf_solver* h, int nsteps) {
   if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
   if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
   const long long l0 = launch_total();
+  void* const uhat = h->uhat;
+  void* const u0 = h->u0;
+  h->graph_parity = state_parity(h);
   h->capturing = true;
   cudaError_t e = cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal);
   int rc = PF_OK;
@@ -1256,6 +1297,9 @@ extern "C" int pf_graph_capture(pf_solver* h, int nsteps) {
     e = cudaStreamEndCapture(h->st, &h->graph);
   }
   h->capturing = false;
+  h->no_swap_next = false;
+  h->uhat = uhat;  // recorded, not run
+  h->u0 = u0;
   h->graph_launches = launch_total() - l0;
   add_launches(-h->graph_launches);  // recorded, not launched
   if (rc) return rc;
@@ -1268,6 +1312,12 @@ extern "C" int pf_graph_capture(pf_solver* h, int nsteps) {
 
 extern "C" int pf_graph_replay(pf_solver* h) {
   if (!h || !h->gexec) return fail(h, PF_ERR_INVALID, "pf_graph_replay: nothing captured");
+  if (state_parity(h) != h->graph_parity) {
+    // steps since the capture left the state in the other buffer: move it back
+    PF_CUDA(h, cudaMemcpyAsync(h->u0, h->uhat, 2 * h->rsz * h->d * h->g.nspec * h->nmem,
+                               cudaMemcpyDeviceToDevice, h->st));
+    std::swap(h->uhat, h->u0);
+  }
   PF_CUDA(h, cudaGraphLaunch(h->gexec, h->st));
   add_launches(h->graph_launches);
   h->step += h->graph_steps;

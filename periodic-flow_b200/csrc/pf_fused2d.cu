@@ -233,7 +233,8 @@ k_q3(UpdateArgs<R> U, const cx<R>* __restrict__ nl, F2 f, const cx<R>* __restric
   double accE = 0.0, accZ = 0.0;
   if (active) {
     const R k1 = (R)(f.ks1 * q);
-    cx<R>* __restrict__ uh = U.uhat + mem.mo;
+    const cx<R>* __restrict__ uh = U.uhat + mem.mo;
+    cx<R>* __restrict__ uo = (U.uout ? U.uout : U.uhat) + mem.mo;  // new state
     cx<R>* __restrict__ u0p = U.u0 + mem.mo;
     const long long ns = f.nspec;
 #pragma unroll
@@ -258,7 +259,7 @@ k_q3(UpdateArgs<R> U, const cx<R>* __restrict__ nl, F2 f, const cx<R>* __restric
         mk_.k[0] = k0; mk_.k[1] = k1;
         mk_.k2 = k0 * k0 + k1 * k1;
         C nv[2] = {v0[e0 + cc], v1[e0 + cc]};
-        update_core<R, 2, NC, NOISE>(U, m, mk_, nv, true, un[cc], u0v[cc], sc, accE, accZ, uh, u0p,
+        update_core<R, 2, NC, NOISE>(U, m, mk_, nv, true, un[cc], u0v[cc], sc, accE, accZ, uo, u0p,
                                      mem.mb);
       }
     }

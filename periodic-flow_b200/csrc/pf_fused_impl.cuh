@@ -907,7 +907,8 @@ k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restr
     const int i1l = q / f.nh, i2 = q - i1l * f.nh;
     const int i1 = SLAB ? i1l + f.sl_i1 : i1l;
     const R k1 = (R)(f.ks1 * kfreq(i1, f.n1)), k2 = (R)(f.ks2 * i2);
-    cx<R>* __restrict__ uh = U.uhat + mem.mo;
+    const cx<R>* __restrict__ uh = U.uhat + mem.mo;
+    cx<R>* __restrict__ uo = (U.uout ? U.uout : U.uhat) + mem.mo;  // new state
     cx<R>* __restrict__ u0p = U.u0 + mem.mo;
     const long long ns = f.nspec;
 #pragma unroll
@@ -934,7 +935,7 @@ k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restr
         C nv[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) nv[a] = nhat(a, i0);
-        update_core<R, 3, NC, NOISE>(U, m, mk_, nv, true, un[cc], u0v[cc], sc, accE, accZ, uh, u0p,
+        update_core<R, 3, NC, NOISE>(U, m, mk_, nv, true, un[cc], u0v[cc], sc, accE, accZ, uo, u0p,
                                      mem.mb);
       }
     }

@@ -31,6 +31,9 @@ template <typename R> struct UpdateArgs {
   // scalars at dscal + mb * kScalCount, E/Z sums at diag + 2 mb, Philox key
   // seed + mb
   long long mstride;
+  // first stage of a step whose state buffers swap roles (or nullptr): the
+  // new state goes here and uhat, left as it is, is the step's u0 (no copy)
+  cx<R>* uout;
 };
 
 template <typename R> struct StokesArgs {

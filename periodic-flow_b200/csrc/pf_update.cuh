@@ -116,10 +116,11 @@ template <typename R> PF_D StageScalars<R> stage_scalars(const UpdateArgs<R>& A,
 }
 
 // Update of mode m from preloaded state un (current) and u0v (start of step)
-// and its unprojected nonlinear term nv (ignored when !has_nl); writes uhat
-// (and u0 at the first stage), adds to the E/Z sums.  NOISE = false compiles
-// the noise path out (noise_mag == 0).  The state of the mode's member is at
-// uh, u0 (A.uhat, A.u0 offset by the member), mb its member index.
+// and its unprojected nonlinear term nv (ignored when !has_nl); writes the new
+// state through uh (and u0 at the first stage unless A.uout takes the new
+// state), adds to the E/Z sums.  NOISE = false compiles the noise path out
+// (noise_mag == 0).  uh, u0: the member's write targets (A.uout or A.uhat,
+// and A.u0, offset by the member), mb its member index.
 template <typename R, int D, int NC, bool NOISE>
 PF_D void update_core(const UpdateArgs<R>& A, long long m, const ModeK<R, D>& mk_,
                       cx<R> (&nv)[D], bool has_nl, cx<R> (&un)[D], const cx<R> (&u0v)[D],
@@ -128,7 +129,7 @@ PF_D void update_core(const UpdateArgs<R>& A, long long m, const ModeK<R, D>& mk
   using C = cx<R>;
   const Geo& g = A.g;
   C xi[D];
-  if (A.save_u0) {
+  if (A.save_u0 && !A.uout) {
 #pragma unroll
     for (int a = 0; a < D; ++a) u0[a * g.nspec + m] = un[a];
   }
@@ -186,7 +187,8 @@ PF_D void update_mode(const UpdateArgs<R>& A, long long m, const ModeK<R, D>& mk
     un[a] = A.uhat[a * A.g.nspec + m];
     u0v[a] = A.save_u0 ? un[a] : A.u0[a * A.g.nspec + m];
   }
-  update_core<R, D, NC, true>(A, m, mk_, nv, has_nl, un, u0v, sc, accE, accZ, A.uhat, A.u0, 0);
+  update_core<R, D, NC, true>(A, m, mk_, nv, has_nl, un, u0v, sc, accE, accZ,
+                              A.uout ? A.uout : A.uhat, A.u0, 0);
 }
 
 }  // namespace pf
