@@ -19,6 +19,11 @@ struct FGeo {
   // buffer (state 3 nspec, nl 3 nlcomp, A 5 t0 c1 c2, B 6 t0 t1 c2 complex
   // values per member); each pass covers all of them in one launch.
   int nmem;
+  // P1's five-row and P2's six-row forms: 1 numbers a CTA's output field
+  // fastest (blockIdx.x = tile * fields + field), so the CTAs of one column
+  // tile run together and their shared input rows are re-read from L2; 0:
+  // the field is blockIdx.y
+  int ilv;
   // Slab decomposition of one box over sl_S slabs (pf_slab.cu; unused by the
   // whole-box passes): slab r holds the spectral rows k1 in [r sl_n1,
   // (r + 1) sl_n1) of every (k0, k2) and, between the two exchanges, the

@@ -183,7 +183,8 @@ k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
   static_assert(!SLAB || (FIVE && !PAD && !MEMB), "slab P1: one field per CTA row, 2/3 rule");
   const int t = threadIdx.x, j = threadIdx.y;
   const int ncols = (SLAB ? f.sl_nc : f.c1) * f.c2;
-  const int q = blockIdx.x * T + t;
+  const int tile = (FIVE && f.ilv) ? (int)blockIdx.x / 5 : (int)blockIdx.x;
+  const int q = tile * T + t;
   const bool active = q < ncols;
   int in_off = 0;
   if (active) {
@@ -218,7 +219,7 @@ k_p1(const cx<R>* __restrict__ uh, cx<R>* __restrict__ A, FGeo f,
   if constexpr (FIVE) {
     // FIVE: block row y makes output field y alone (u0, u1, u2, D1, D2) with
     // one line buffer; the derivative rows re-read u1, u2
-    const int fld = blockIdx.y;
+    const int fld = f.ilv ? (int)blockIdx.x - tile * 5 : (int)blockIdx.y;
     const int c = fld < 3 ? fld : fld - 2;
     C w[E];
 #pragma unroll
@@ -296,7 +297,8 @@ k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
   }
   const int t = threadIdx.x, j = threadIdx.y;
   const int ncols = f.t0 * f.c2;
-  const int q = blockIdx.x * T + t;
+  const int tile = (SIX && f.ilv) ? (int)blockIdx.x / 6 : (int)blockIdx.x;
+  const int q = tile * T + t;
   const bool active = q < ncols;
   int in_base = 0, out_base = 0;
   R k2 = 0;
@@ -350,7 +352,8 @@ k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
     // (omega fields read their two inputs): one FFT per CTA, fewer registers,
     // at the cost of re-reading u0, u1, u2
     C w[E];
-    switch (blockIdx.y) {
+    const int row = f.ilv ? (int)blockIdx.x - tile * 6 : (int)blockIdx.y;
+    switch (row) {
       case 0:  // omega0 = i (k1 u2 - k2 u1)
 #pragma unroll
         for (int e = 0; e < E; ++e) w[e] = cmuli(csub(cscale(ld(2, e), k1(e)), cscale(ld(1, e), k2)));
@@ -360,7 +363,7 @@ k_p2(const cx<R>* __restrict__ A, cx<R>* __restrict__ B, FGeo f,
       case 1:
       case 2:
       case 5: {  // u1, u2, u0
-        const int fld = blockIdx.y == 5 ? 0 : (int)blockIdx.y;
+        const int fld = row == 5 ? 0 : row;
 #pragma unroll
         for (int e = 0; e < E; ++e) w[e] = ld(fld, e);
         fft<N, E, +1>(w, j, tw, smf, sync);
@@ -1075,7 +1078,8 @@ static cudaError_t p1five_run(FusedPlan* p, const cx<R>* uh, cudaStream_t st) {
   const size_t sm = strided_smem<R, N, E, T, PAD>();
   cudaError_t e = set_smem(k_p1<R, N, E, T, MB, PAD, true, MEMB>, sm);
   if (e != cudaSuccess) return e;
-  const dim3 grid((unsigned)((ncols + T - 1) / T), 5, MEMB ? (unsigned)p->f.nmem : 1u);
+  const unsigned tiles = (unsigned)((ncols + T - 1) / T);
+  const dim3 grid(p->f.ilv ? 5 * tiles : tiles, p->f.ilv ? 1u : 5u, MEMB ? (unsigned)p->f.nmem : 1u);
   k_p1<R, N, E, T, MB, PAD, true, MEMB><<<grid, dim3(T, G), sm, st>>>(uh, (cx<R>*)p->A, p->f, tw);
   return launched();
 }
@@ -1121,7 +1125,8 @@ static cudaError_t p2six_run(FusedPlan* p, cudaStream_t st) {
   const size_t sm = strided_smem<R, N, E, T, PAD>();
   cudaError_t e = set_smem(k_p2<R, N, E, T, MB, PAD, true, MEMB>, sm);
   if (e != cudaSuccess) return e;
-  const dim3 grid((unsigned)((ncols + T - 1) / T), 6, MEMB ? (unsigned)p->f.nmem : 1u);
+  const unsigned tiles = (unsigned)((ncols + T - 1) / T);
+  const dim3 grid(p->f.ilv ? 6 * tiles : tiles, p->f.ilv ? 1u : 6u, MEMB ? (unsigned)p->f.nmem : 1u);
   k_p2<R, N, E, T, MB, PAD, true, MEMB><<<grid, dim3(T, G), sm, st>>>(
       (const cx<R>*)p->A, (cx<R>*)p->B, p->f, tw);
   return launched();

@@ -407,6 +407,7 @@ int alloc_slab(pf_slab* h, int r, SlabBuf& b) {
   fc.nlrow = b.L.n1s * g.nh;
   fc.nlcomp = ns;
   fc.nmem = 1;
+  fc.ilv = 0;  // slab P1 numbers its fields by blockIdx.y
   // P4: the pencil plan's geometry
   b.fp = b.pp->f;
   for (FGeo* f : {&fc, &b.fp}) {
