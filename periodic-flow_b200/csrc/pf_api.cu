@@ -557,9 +557,16 @@ static int step_impl(pf_solver* h, int nsteps) {
   int done = 0;
   // noise-free runs without history or timer: one recorded step graph per
   // step (the step's launches cost one graph launch; dt, time and the CFL
-  // reduction live in device scalars, so the graph is step-independent)
+  // reduction live in device scalars, so the graph is step-independent),
+  // unless the caller's stream is being captured itself
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(h->st, &cap) != cudaSuccess) {
+    cudaGetLastError();
+    cap = cudaStreamCaptureStatusActive;
+  }
   const bool graphable = !stokes_fast && h->auto_graph && !injected && noise_src(h) == kNoiseNone &&
-                         !h->record_hist && h->tpass < 0 && nsteps >= 2;
+                         !h->record_hist && h->tpass < 0 && nsteps >= 1 &&
+                         cap == cudaStreamCaptureStatusNone;
   if (graphable) {
     for (; done < nsteps; ++done) {
       const int par = state_parity(h);

@@ -90,7 +90,7 @@ class Realisations:
     of them (C-ABI ``pf_create_members``).  Each member keeps its own dt (CFL),
     time and forcing-band energy; member ``m`` draws Philox noise with key
     ``seed + m``, so it equals a ``Solver`` created with that seed.
-    ``step(n)`` with n >= 2 replays a recorded one-step CUDA graph for
+    ``step(n)`` replays a recorded one-step CUDA graph for
     noise-free runs, as a single solver does.
     """
 
