@@ -1,4 +1,4 @@
-// Register-resident Stockham FFT engine (power-of-two lengths).
+// Register-resident Stockham FFT engine (lengths 2^b and 3 * 2^b).
 //
 // A line of N complex values is owned by G = N / E threads; thread j holds
 // x[j + G*e] for e in [0, E) ("natural strided" mapping).  Each radix-R stage
@@ -140,17 +140,20 @@ template <int R, int DIR, typename C> PF_D void dft(C* v) {
 }
 
 // ---- stage plan -------------------------------------------------------------
-// N = 2^b or 3 * 2^b.  A factor 3 is done first as a radix-3 stage (E must
-// then be a multiple of 3); the power-of-two part takes greedy radices E2,
-// E2, ..., remainder with E2 the power-of-two part of E.  Ns(s) = product of
-// earlier radices.  Every radix divides E.
-template <int N, int E> struct Plan {
+// N = 2^b or 3 * 2^b.  A factor 3 goes into the first stage (E a multiple
+// of 3): with M3 a radix 3 R2 DFT in registers (dft3x: R2 = min(E2, N / 3)),
+// without it a radix-3 stage of its own; the rest of the power-of-two part
+// takes greedy radices E2, E2, ..., remainder with E2 the power-of-two part
+// of E.  Ns(s) = product of earlier radices.  Every radix divides E.
+template <int N, int E, bool M3 = true> struct Plan {
   static constexpr int P3 = (N % 3 == 0) ? 1 : 0;
   static constexpr int E2 = (E % 3 == 0) ? E / 3 : E;
   static_assert(!P3 || E % 3 == 0, "a radix-3 stage needs E divisible by 3");
+  // first radix (the factor 3)
+  static constexpr int R0 = P3 ? (M3 ? 3 * ((N / 3) < E2 ? (N / 3) : E2) : 3) : 1;
   static constexpr int radix(int s) {
-    if (P3 && s == 0) return 3;
-    int rem = P3 ? N / 3 : N, r = 1;
+    if (P3 && s == 0) return R0;
+    int rem = P3 ? N / R0 : N, r = 1;
     for (int t = P3; t <= s; ++t) { r = rem < E2 ? rem : E2; rem /= r; }
     return r;
   }
@@ -165,6 +168,40 @@ template <int N, int E> struct Plan {
     return s;
   }
 };
+
+// Radix R = 3 R2 in registers (Cooley-Tukey, 3 x R2): 3-point DFTs over n1
+// of v[R2 n1 + n2], twiddles W_R^(k1 n2), R2-point DFTs over n2; output k =
+// k1 + 3 k2 in natural order.  W_R^m = exp(DIR 2 pi i m / R) is entry
+// m N / R of the length-N table (conjugated for DIR > 0).
+template <int N, int R2, int DIR, typename C>
+PF_D void dft3x(C* v, const C* __restrict__ tw) {
+  constexpr int R = 3 * R2;
+  static_assert(N % R == 0, "the table of length N holds W_R");
+  C y[3][R2];
+#pragma unroll
+  for (int n2 = 0; n2 < R2; ++n2) {
+    C a = v[n2], b = v[R2 + n2], c = v[2 * R2 + n2];
+    dft3<DIR>(a, b, c);
+    y[0][n2] = a;
+    y[1][n2] = b;
+    y[2][n2] = c;
+  }
+#pragma unroll
+  for (int k1 = 1; k1 < 3; ++k1) {
+#pragma unroll
+    for (int n2 = 1; n2 < R2; ++n2) {
+      C w = ldtw(tw + (k1 * n2) * (N / R));
+      if (DIR > 0) w.y = -w.y;
+      y[k1][n2] = cmul(y[k1][n2], w);
+    }
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < 3; ++k1) {
+    dft<R2, DIR>(y[k1]);
+#pragma unroll
+    for (int k2 = 0; k2 < R2; ++k2) v[k1 + 3 * k2] = y[k1][k2];
+  }
+}
 
 // One Stockham stage on the thread's E registers.  Returns with v holding the
 // stage output at positions given by dst(); the caller exchanges or stops.
@@ -188,7 +225,8 @@ PF_D void stage_compute(C (&v)[E], int j, const C* __restrict__ tw) {
         b[r] = cmul(b[r], w);
       }
     }
-    dft<R, DIR>(b);
+    if constexpr (R % 3 == 0 && R > 3) dft3x<N, R / 3, DIR>(b, tw);
+    else dft<R, DIR>(b);
 #pragma unroll
     for (int r = 0; r < R; ++r) v[q + r * Q] = b[r];
   }
@@ -203,10 +241,10 @@ template <int N, int E, int R, int NS> PF_D int stage_dst(int j, int e) {
   return (jv / NS) * NS * R + (jv % NS) + r * NS;
 }
 
-template <int N, int E, int DIR, int s, int S, typename C, typename SMF, typename SYNCF>
+template <int N, int E, int DIR, int s, int S, bool M3, typename C, typename SMF, typename SYNCF>
 PF_D void fft_stages(C (&v)[E], int j, const C* tw, SMF& sm, SYNCF& sync) {
   if constexpr (s < S) {
-    using P = Plan<N, E>;
+    using P = Plan<N, E, M3>;
     constexpr int R = P::radix(s);
     constexpr int NS = P::ns(s);
     stage_compute<N, E, R, NS, DIR>(v, j, tw);
@@ -219,19 +257,19 @@ PF_D void fft_stages(C (&v)[E], int j, const C* tw, SMF& sm, SYNCF& sync) {
       for (int e = 0; e < E; ++e) v[e] = sm(j + G * e);
       sync();
     }
-    fft_stages<N, E, DIR, s + 1, S>(v, j, tw, sm, sync);
+    fft_stages<N, E, DIR, s + 1, S, M3>(v, j, tw, sm, sync);
   }
 }
 
 // Full FFT.  SM(pos) -> C& addresses the exchange buffer of this line; SYNC()
 // synchronises all threads sharing the buffer.  Called by every thread of the
 // group (no divergence around it).
-template <int N, int E, int DIR, typename C, typename SMF, typename SYNCF>
+template <int N, int E, int DIR, bool M3 = true, typename C, typename SMF, typename SYNCF>
 PF_D void fft(C (&v)[E], int j, const C* __restrict__ tw, SMF sm, SYNCF sync) {
-  using P = Plan<N, E>;
+  using P = Plan<N, E, M3>;
   constexpr int S = P::stages();
   static_assert(N % E == 0, "E divides N");
-  fft_stages<N, E, DIR, 0, S>(v, j, tw, sm, sync);
+  fft_stages<N, E, DIR, 0, S, M3>(v, j, tw, sm, sync);
 }
 
 }  // namespace pf

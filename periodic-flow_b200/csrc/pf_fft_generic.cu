@@ -46,7 +46,7 @@ k_fft_strided(cx<R>* __restrict__ data, long long ncols, long long ntotal,
 #pragma unroll
   for (int e = 0; e < E; ++e)
     v[e] = active ? data[base + (long long)(j + G * e) * line_stride] : czero<C>();
-  fft<N, E, DIR>(v, j, tw, [&](int pos) -> C& { return sm[pos * T + t]; },
+  fft<N, E, DIR, false>(v, j, tw, [&](int pos) -> C& { return sm[pos * T + t]; },
                  [] { __syncthreads(); });
   if (active) {
 #pragma unroll
@@ -88,8 +88,8 @@ k_c2r_last(const cx<R>* __restrict__ in, R* __restrict__ out, long long nlines,
     v[e] = z;
   }
   auto smf = [&](int pos) -> C& { return sm[pos + (pos >> SH)]; };
-  if constexpr (G <= 32) fft<N, E, +1>(v, j, tw, smf, [] { __syncwarp(); });
-  else fft<N, E, +1>(v, j, tw, smf, [] { __syncthreads(); });
+  if constexpr (G <= 32) fft<N, E, +1, false>(v, j, tw, smf, [] { __syncwarp(); });
+  else fft<N, E, +1, false>(v, j, tw, smf, [] { __syncthreads(); });
   R* oa = out + la * out_stride;
   R* ob = out + lb * out_stride;
 #pragma unroll
@@ -126,7 +126,7 @@ k_r2c_last(const R* __restrict__ in, cx<R>* __restrict__ out, long long nlines,
   }
   auto smf = [&](int pos) -> C& { return sm[pos + (pos >> SH)]; };
   auto sync = [] { if constexpr (G <= 32) __syncwarp(); else __syncthreads(); };
-  fft<N, E, -1>(v, j, tw, smf, sync);
+  fft<N, E, -1, false>(v, j, tw, smf, sync);
 #pragma unroll
   for (int e = 0; e < E; ++e) smf(j + G * e) = v[e];
   sync();
@@ -169,7 +169,7 @@ static cudaError_t launch_strided(cx<R>* data, int dir, long long ncols, long lo
   dim3 grid((unsigned)((ntotal + TN::T - 1) / TN::T));
   // exchange buffer whenever the plan has more than one stage (a 3 * 2^b
   // length with one thread per line still exchanges between its stages)
-  size_t sm = Plan<N, TN::E>::stages() > 1 ? sizeof(cx<R>) * N * TN::T : 0;
+  size_t sm = Plan<N, TN::E, false>::stages() > 1 ? sizeof(cx<R>) * N * TN::T : 0;
   const int us = scale != 1.0;
   cudaError_t e;
   if (dir < 0) {
