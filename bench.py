@@ -580,6 +580,8 @@ def run_padded(args, uh0, peak):
         sol = make_solver(n, dealias="3/2", fused=fused)
         ss = sol.space_solver
         ss.initialize_velocity(uh0, "fourier")
+        if fused and not args.no_autotune:
+            out["launch_variants"] = ss.autotune()
         ss.step(2)
         torch.cuda.synchronize()
         k = args.padded_steps
