@@ -1,9 +1,9 @@
-"""The baseline configurations' FP32 and FP64 results against the FP64 oracle.
+"""The benchmark workloads' FP32 and FP64 results against the FP64 oracle.
 
 * forced-turbulence headline at its full size (256^3 FP32, seed-1 field, band
   forcing, RK3 with CFL dt) one step from the same initial field;
 * the shell spectrum diagnostic against oracle.spectrum;
-* configuration 2 (2D thermal Stokes 256^2, explicit PC, as specified) with
+* the 2D thermal Stokes workload (256^2, nu 0.1, explicit PC, dt 0.01) with
   the reference's NumPy draws injected into both codes, FP32 and FP64.
 
 Tolerances (relative L2 over all modes): FP32 1e-5, FP64 1e-12.
