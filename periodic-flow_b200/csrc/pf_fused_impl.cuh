@@ -852,9 +852,11 @@ k_p4(cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
 // loaded before any of its stores.
 // SLAB: the columns of one slab's k1 rows [sl_i1, sl_i1 + sl_n1) (state and
 // nl in the slab's layout; wavenumbers and noise sites of the whole box).
+// MB5 > 0: at least MB5 CTAs per SM (register cap) instead of the default.
 template <typename R, int N, int NC, bool NOISE, int CHU, bool PAD, bool MEMB = false,
-          bool SLAB = false>
-__global__ void __launch_bounds__(TuneU<N, R>::T * TuneU<N, R>::G, sizeof(R) == 8 ? 1 : 2)
+          bool SLAB = false, int MB5 = 0>
+__global__ void __launch_bounds__(TuneU<N, R>::T * TuneU<N, R>::G,
+                                  MB5 ? MB5 : (sizeof(R) == 8 ? 1 : 2))
 k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
   constexpr int E = TuneU<N, R>::E, G = TuneU<N, R>::G, T = TuneU<N, R>::T;
   const Member mem = member_of(U, MEMB ? (int)blockIdx.y : 0);  // member blockIdx.y
@@ -1275,10 +1277,16 @@ static cudaError_t p3_n(FusedPlan* p, cx<R>* nl, unsigned long long* maxbits, cu
 }
 
 // the single-box or the member form of P5
-template <typename R, bool PAD, int N, int CH, int NC, bool NOISE>
+template <typename R, bool PAD, int N, int CH, int NC, bool NOISE, int MB5 = 0>
 static cudaError_t p5_go(FusedPlan* p, const UpdateArgs<R>& U, const cx<R>* nl, dim3 grid,
                          dim3 block, size_t sm, const cx<R>* tw, cudaStream_t st) {
   cudaError_t e;
+  if constexpr (MB5 > 0) {  // one box
+    e = set_smem(k_p5<R, N, NC, NOISE, CH, PAD, false, false, MB5>, sm);
+    if (e != cudaSuccess) return e;
+    k_p5<R, N, NC, NOISE, CH, PAD, false, false, MB5><<<grid, block, sm, st>>>(U, nl, p->f, tw);
+    return cudaSuccess;
+  }
   if (p->f.nmem > 1) {
     e = set_smem(k_p5<R, N, NC, NOISE, CH, PAD, true>, sm);
     if (e != cudaSuccess) return e;
@@ -1291,7 +1299,7 @@ static cudaError_t p5_go(FusedPlan* p, const UpdateArgs<R>& U, const cx<R>* nl, 
   return cudaSuccess;
 }
 
-template <typename R, bool PAD, int N, int CH>
+template <typename R, bool PAD, int N, int CH, int MB5 = 0>
 static cudaError_t p5_run(FusedPlan* p, const UpdateArgs<R>& U, int ncomp, const cx<R>* nl,
                           cudaStream_t st) {
   using TN = TuneU<N, R>;
@@ -1300,15 +1308,17 @@ static cudaError_t p5_run(FusedPlan* p, const UpdateArgs<R>& U, int ncomp, const
   const size_t sm = sizeof(cx<R>) * 3 * N * TN::T;
   const dim3 grid((unsigned)((ncols + TN::T - 1) / TN::T), (unsigned)p->f.nmem),
       block(TN::T, TN::G);
+  if (MB5 > 0 && p->f.nmem > 1) return cudaErrorInvalidValue;
   cudaError_t e;
-  if (U.noise_src == kNoiseNone) e = p5_go<R, PAD, N, CH, 3, false>(p, U, nl, grid, block, sm, tw, st);
-  else if (ncomp == 9) e = p5_go<R, PAD, N, CH, 9, true>(p, U, nl, grid, block, sm, tw, st);
-  else e = p5_go<R, PAD, N, CH, 3, true>(p, U, nl, grid, block, sm, tw, st);
+  if (U.noise_src == kNoiseNone) e = p5_go<R, PAD, N, CH, 3, false, MB5>(p, U, nl, grid, block, sm, tw, st);
+  else if (ncomp == 9) e = p5_go<R, PAD, N, CH, 9, true, MB5>(p, U, nl, grid, block, sm, tw, st);
+  else e = p5_go<R, PAD, N, CH, 3, true, MB5>(p, U, nl, grid, block, sm, tw, st);
   return e != cudaSuccess ? e : launched();
 }
 
 // Variant 0 keeps the state loads of 4 rows per thread in flight (FP64: 2);
-// 1, 2 (FP32, n0 = 256) use 2 and 8.
+// 1, 2 (FP32, n0 = 256) use 2 and 8; FP64 from 128 points runs two CTAs per
+// SM unless variant 4.
 template <typename R, int N, bool PAD>
 static cudaError_t p5_n(FusedPlan* p, const UpdateArgs<R>& U, int ncomp, const cx<R>* nl,
                         cudaStream_t st) {
@@ -1318,6 +1328,13 @@ static cudaError_t p5_n(FusedPlan* p, const UpdateArgs<R>& U, int ncomp, const c
       case 2: return p5_run<R, PAD, 256, 8>(p, U, ncomp, nl, st);
       default: break;
     }
+  }
+  if constexpr (sizeof(R) == 8 && !PAD && N >= 128) {
+    // FP64, one box, no noise: two CTAs per SM (registers capped at 128, 16
+    // bytes spilled at 256) instead of one at 158 registers -- 3.54 against
+    // 3.76 ms per RK3 step at 256^3; variant 4 keeps one CTA per SM
+    if (p->var[5] != 4 && p->f.nmem == 1 && U.noise_src == kNoiseNone)
+      return p5_run<R, PAD, N, 2, 2>(p, U, ncomp, nl, st);
   }
   return p5_run<R, PAD, N, sizeof(R) == 8 ? 2 : 4>(p, U, ncomp, nl, st);
 }
