@@ -269,23 +269,30 @@ cudaError_t fused_autotune(FusedPlan* p, const void* uhat, void* nl, cudaStream_
     const std::vector<int> cand = candidates(p, pass, is384);
     int* slot = is384 ? &p->var384[pass] : &p->var[pass];
     const int keep = *slot;
-    float best = 1e30f;
-    int pick = keep;
-    for (size_t i = 0; i < cand.size() && err == cudaSuccess; ++i) {
-      *slot = cand[i];
-      err = chain();  // warm-up, first use of the variant
-      if (err != cudaSuccess) break;
-      float ms = 0.f;
-      cudaEventRecord(e0, st);
-      for (int r = 0; r < 4 && err == cudaSuccess; ++r) err = chain();
-      cudaEventRecord(e1, st);
-      if (err == cudaSuccess) err = cudaEventSynchronize(e1);
-      if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
-      if (err == cudaSuccess && ms < best) {
-        best = ms;
-        pick = cand[i];
+    // three rounds over all candidates, each candidate's best round counts
+    // (variants a few microseconds apart are otherwise picked by noise)
+    std::vector<float> best(cand.size(), 1e30f);
+    for (int round = 0; round < 3 && err == cudaSuccess; ++round) {
+      for (size_t i = 0; i < cand.size() && err == cudaSuccess; ++i) {
+        *slot = cand[i];
+        err = chain();  // warm-up: first use of the variant, L2 state of the chain
+        if (err != cudaSuccess) break;
+        float ms = 0.f;
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < 4 && err == cudaSuccess; ++r) err = chain();
+        cudaEventRecord(e1, st);
+        if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+        if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+        if (err == cudaSuccess && ms < best[i]) best[i] = ms;
       }
     }
+    int pick = keep;
+    float bmin = 1e30f;
+    for (size_t i = 0; i < cand.size(); ++i)
+      if (best[i] < bmin) {
+        bmin = best[i];
+        pick = cand[i];
+      }
     *slot = err == cudaSuccess ? pick : keep;
   }
   cudaEventDestroy(e0);
