@@ -392,8 +392,8 @@ static int step_generic(pf_solver* h) {
     void* const cur = s == 0 ? old_state : new_state;  // the stage's input state
     if (h->cfg.is_nonlinear) {
       if (use_fused) {
-        if (s == 0 && cfl)
-          PF_CUDA(h, cudaMemsetAsync(h->maxbits, 0, sizeof(unsigned long long) * h->nact, h->st));
+        // (the CFL words start at zero: zeroed at creation, and k_set_dt resets
+        // them after reading)
         for (int p = 1; p <= 4; ++p) {
           tmark(h, PF_PASS_FUSED_P1 + p - 1);
           cudaError_t fe = fused_pass(h->fused, p, cur, h->nl,

@@ -89,7 +89,8 @@ template <typename R>
 cudaError_t launch_cross(R* u, const R* w, const Geo& g, unsigned long long* maxbits, cudaStream_t st);
 // The per-step scalar kernels cover nmem members (dscal, maxbits, u strided
 // by kScalCount, 1 and d nspec per member).
-cudaError_t launch_set_dt(double* dscal, const unsigned long long* maxbits, double cfl, cudaStream_t st,
+// (reads each member's CFL maximum and resets the word to zero)
+cudaError_t launch_set_dt(double* dscal, unsigned long long* maxbits, double cfl, cudaStream_t st,
                           int nmem = 1);
 // 3/2 rule: N-grid spectrum (or its curl) onto the M = 3N/2 grid, and back
 template <typename R>

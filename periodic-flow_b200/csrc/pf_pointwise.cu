@@ -181,12 +181,13 @@ __global__ void k_cross(R* __restrict__ u, const R* __restrict__ w, Geo g,
   }
 }
 
-// dscal[dt] = cfl / max, from the double bits written by k_cross (one
-// thread per member)
-__global__ void k_set_dt(double* dscal, const unsigned long long* maxbits, double cfl, int nmem) {
+// dscal[dt] = cfl / max, from the double bits written by k_cross or P3 (one
+// thread per member); the word is reset to zero for the next maximum
+__global__ void k_set_dt(double* dscal, unsigned long long* maxbits, double cfl, int nmem) {
   for (int m = threadIdx.x; m < nmem; m += blockDim.x) {
     double* d = dscal + (long long)m * kScalCount;
     const double mx = __longlong_as_double((long long)maxbits[m]);
+    maxbits[m] = 0ull;
     if (mx > 0.0) d[kScalDt] = cfl / mx;
     d[kScalTime] += d[kScalDt];
   }
@@ -205,7 +206,9 @@ __global__ void k_advance_time(double* dscal, int n, int nmem) {
 // index s when the whole axis is needed, else to wavenumber s - K (mod n).
 struct BandBox { int cnt[3], K[3], full[3]; long long total; };
 
-template <typename R, int D>
+// single: one CTA per member stores the sum (no zeroed slot needed);
+// otherwise CTAs add into a zeroed slot.
+template <typename R, int D, bool SINGLE = false>
 __global__ void k_band_energy(const cx<R>* __restrict__ u, Geo g, double kf2, BandBox bx,
                               double* dscal) {
   // member blockIdx.y of boxes laid out one after another
@@ -234,7 +237,8 @@ __global__ void k_band_energy(const cx<R>* __restrict__ u, Geo g, double kf2, Ba
       acc += 0.5 * half_weight(g, q.ix) * e;
     }
   }
-  block_add2(acc, 0.0, dscal + kScalBandE);
+  if constexpr (SINGLE) block_store2(acc, 0.0, dscal + kScalBandE);
+  else block_add2(acc, 0.0, dscal + kScalBandE);
 }
 
 template <typename R, int D>
@@ -445,7 +449,7 @@ cudaError_t launch_cross(R* u, const R* w, const Geo& g, unsigned long long* max
   return launched();
 }
 
-cudaError_t launch_set_dt(double* dscal, const unsigned long long* maxbits, double cfl,
+cudaError_t launch_set_dt(double* dscal, unsigned long long* maxbits, double cfl,
                           cudaStream_t st, int nmem) {
   k_set_dt<<<1, nmem < 256 ? (nmem < 32 ? 32 : nmem) : 256, 0, st>>>(dscal, maxbits, cfl, nmem);
   return launched();
@@ -459,10 +463,6 @@ cudaError_t launch_advance_time(double* dscal, int n, cudaStream_t st, int nmem)
 template <typename R>
 cudaError_t launch_band_energy(const cx<R>* u, const Geo& g, double kf2, double* dscal,
                                cudaStream_t st, int nmem) {
-  // zero each member's band-energy slot (dscal rows of kScalCount doubles)
-  cudaError_t e = cudaMemset2DAsync(dscal + kScalBandE, sizeof(double) * kScalCount, 0,
-                                    sizeof(double), (size_t)nmem, st);
-  if (e != cudaSuccess) return e;
   BandBox bx;
   bx.total = 1;
   const double kf = sqrt(kf2);
@@ -480,6 +480,16 @@ cudaError_t launch_band_energy(const cx<R>* u, const Geo& g, double kf2, double*
     }
     bx.total *= bx.cnt[a];
   }
+  if (bx.total <= 64 * kBlock) {  // one CTA per member stores its sum
+    const dim3 grid(1, (unsigned)nmem);
+    if (g.dim == 3) k_band_energy<R, 3, true><<<grid, kBlock, 0, st>>>(u, g, kf2, bx, dscal);
+    else k_band_energy<R, 2, true><<<grid, kBlock, 0, st>>>(u, g, kf2, bx, dscal);
+    return launched();
+  }
+  // zero each member's band-energy slot (dscal rows of kScalCount doubles)
+  cudaError_t e = cudaMemset2DAsync(dscal + kScalBandE, sizeof(double) * kScalCount, 0,
+                                    sizeof(double), (size_t)nmem, st);
+  if (e != cudaSuccess) return e;
   const dim3 grid(grid_for(bx.total), (unsigned)nmem);
   if (g.dim == 3) k_band_energy<R, 3><<<grid, kBlock, 0, st>>>(u, g, kf2, bx, dscal);
   else k_band_energy<R, 2><<<grid, kBlock, 0, st>>>(u, g, kf2, bx, dscal);

@@ -8,9 +8,11 @@
 
 namespace pf {
 
-// FP64 block reduction of two partial sums into gl[0], gl[1].  Every thread
-// of the block must call it.
-PF_D void block_add2(double a, double b, double* gl) {
+// FP64 block reduction of two partial sums, stored into gl[0], gl[1] by one
+// thread (block_store2: the block's own slots) or added to them atomically
+// (block_add2).  Every thread of the block must call it.
+template <bool ADD>
+PF_D void block_reduce2(double a, double b, double* gl) {
   __shared__ double sa[32], sb[32];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -31,9 +33,15 @@ PF_D void block_add2(double a, double b, double* gl) {
       a += __shfl_xor_sync(0xffffffffu, a, o);
       b += __shfl_xor_sync(0xffffffffu, b, o);
     }
-    if (l == 0) { atomicAdd(gl, a); atomicAdd(gl + 1, b); }
+    if (l == 0) {
+      if constexpr (ADD) { atomicAdd(gl, a); atomicAdd(gl + 1, b); }
+      else { gl[0] = a; gl[1] = b; }
+    }
   }
 }
+PF_D void block_store2(double a, double b, double* gl) { block_reduce2<false>(a, b, gl); }
+
+PF_D void block_add2(double a, double b, double* gl) { block_reduce2<true>(a, b, gl); }
 
 // Member mb of a launch over boxes laid out member after member: its state
 // is at uhat / u0 + mo (mo = mb * mstride), its scalars at dscal + mb *
