@@ -853,15 +853,18 @@ k_p4(cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
 // SLAB: the columns of one slab's k1 rows [sl_i1, sl_i1 + sl_n1) (state and
 // nl in the slab's layout; wavenumbers and noise sites of the whole box).
 // MB5 > 0: at least MB5 CTAs per SM (register cap) instead of the default.
+// S0: the first stage of a step (u0 is the state itself, nothing to load for
+// it), with 8 rows of state loads in flight.
 template <typename R, int N, int NC, bool NOISE, int CHU, bool PAD, bool MEMB = false,
-          bool SLAB = false, int MB5 = 0>
+          bool SLAB = false, int MB5 = 0, bool S0 = false>
 __global__ void __launch_bounds__(TuneU<N, R>::T * TuneU<N, R>::G,
                                   MB5 ? MB5 : (sizeof(R) == 8 ? 1 : 2))
 k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restrict__ tw) {
   constexpr int E = TuneU<N, R>::E, G = TuneU<N, R>::G, T = TuneU<N, R>::T;
   const Member mem = member_of(U, MEMB ? (int)blockIdx.y : 0);  // member blockIdx.y
   if (MEMB) nl += (long long)blockIdx.y * 3 * f.nlcomp;
-  constexpr int CH = E < CHU ? E : CHU;  // rows per thread whose state loads are in flight
+  // rows per thread whose state loads are in flight
+  constexpr int CH = S0 ? (E < 8 ? E : 8) : (E < CHU ? E : CHU);
   using C = cx<R>;
   extern __shared__ __align__(16) unsigned char smraw[];
   C* S = reinterpret_cast<C*>(smraw);
@@ -925,7 +928,7 @@ k_p5(UpdateArgs<R> U, const cx<R>* __restrict__ nl, FGeo f, const cx<R>* __restr
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
           un[cc][a] = uh[a * ns + m];
-          u0v[cc][a] = U.save_u0 ? un[cc][a] : u0p[a * ns + m];
+          u0v[cc][a] = (S0 || U.save_u0) ? un[cc][a] : u0p[a * ns + m];
         }
       }
 #pragma unroll
@@ -1277,10 +1280,16 @@ static cudaError_t p3_n(FusedPlan* p, cx<R>* nl, unsigned long long* maxbits, cu
 }
 
 // the single-box or the member form of P5
-template <typename R, bool PAD, int N, int CH, int NC, bool NOISE, int MB5 = 0>
+template <typename R, bool PAD, int N, int CH, int NC, bool NOISE, int MB5 = 0, bool S0 = false>
 static cudaError_t p5_go(FusedPlan* p, const UpdateArgs<R>& U, const cx<R>* nl, dim3 grid,
                          dim3 block, size_t sm, const cx<R>* tw, cudaStream_t st) {
   cudaError_t e;
+  if constexpr (S0) {  // one box, first stage
+    e = set_smem(k_p5<R, N, NC, NOISE, CH, PAD, false, false, MB5, true>, sm);
+    if (e != cudaSuccess) return e;
+    k_p5<R, N, NC, NOISE, CH, PAD, false, false, MB5, true><<<grid, block, sm, st>>>(U, nl, p->f, tw);
+    return cudaSuccess;
+  }
   if constexpr (MB5 > 0) {  // one box
     e = set_smem(k_p5<R, N, NC, NOISE, CH, PAD, false, false, MB5>, sm);
     if (e != cudaSuccess) return e;
@@ -1299,7 +1308,7 @@ static cudaError_t p5_go(FusedPlan* p, const UpdateArgs<R>& U, const cx<R>* nl, 
   return cudaSuccess;
 }
 
-template <typename R, bool PAD, int N, int CH, int MB5 = 0>
+template <typename R, bool PAD, int N, int CH, int MB5 = 0, bool S0 = false>
 static cudaError_t p5_run(FusedPlan* p, const UpdateArgs<R>& U, int ncomp, const cx<R>* nl,
                           cudaStream_t st) {
   using TN = TuneU<N, R>;
@@ -1308,9 +1317,9 @@ static cudaError_t p5_run(FusedPlan* p, const UpdateArgs<R>& U, int ncomp, const
   const size_t sm = sizeof(cx<R>) * 3 * N * TN::T;
   const dim3 grid((unsigned)((ncols + TN::T - 1) / TN::T), (unsigned)p->f.nmem),
       block(TN::T, TN::G);
-  if (MB5 > 0 && p->f.nmem > 1) return cudaErrorInvalidValue;
+  if ((MB5 > 0 || S0) && p->f.nmem > 1) return cudaErrorInvalidValue;
   cudaError_t e;
-  if (U.noise_src == kNoiseNone) e = p5_go<R, PAD, N, CH, 3, false, MB5>(p, U, nl, grid, block, sm, tw, st);
+  if (U.noise_src == kNoiseNone) e = p5_go<R, PAD, N, CH, 3, false, MB5, S0>(p, U, nl, grid, block, sm, tw, st);
   else if (ncomp == 9) e = p5_go<R, PAD, N, CH, 9, true, MB5>(p, U, nl, grid, block, sm, tw, st);
   else e = p5_go<R, PAD, N, CH, 3, true, MB5>(p, U, nl, grid, block, sm, tw, st);
   return e != cudaSuccess ? e : launched();
@@ -1327,6 +1336,12 @@ static cudaError_t p5_n(FusedPlan* p, const UpdateArgs<R>& U, int ncomp, const c
       case 1: return p5_run<R, PAD, 256, 2>(p, U, ncomp, nl, st);
       case 2: return p5_run<R, PAD, 256, 8>(p, U, ncomp, nl, st);
       default: break;
+    }
+    if constexpr (!PAD) {
+      // first stage, one box, no noise: 8 rows of state loads in flight
+      // (variant 5 keeps the general form)
+      if (p->var[5] != 5 && U.save_u0 && p->f.nmem == 1 && U.noise_src == kNoiseNone)
+        return p5_run<R, PAD, 256, 4, 0, true>(p, U, ncomp, nl, st);
     }
   }
   if constexpr (sizeof(R) == 8 && !PAD && N >= 128) {
